@@ -1,0 +1,426 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 Landau-Lifshitz MD path.
+
+Headline workload (one bench step): the batched 2DCS delay scan on the
+1152-spin Kitaev honeycomb (24x24x1, K=-1, Gamma=0.25, Gamma'=-0.02, no static
+field), FP64 RK4 dt=0.01 for 2x10^4 steps from T_start=-5, 256 delays
+tau_k = 100 k/255, each a pump-only, probe-only and pump+probe trajectory
+(768 trajectories) in ONE launch; Gaussian pulses amp 0.5, width 0.5,
+freq 0, direction (1,1,1)/sqrt3 on both sublattices (rotated by the
+sublattice frame like Lattice::set_pulse); initial state zigzag +
+Gaussian tilt sigma=0.05 (seed 2), renormalised; M_af/M_local/M_global and
+E/N reduced every step.
+
+Metric: spin*RK4-steps/s = B * N * steps / time (whole job, all GPUs).
+  value      device-resident inputs, CUDA events on the launching stream;
+  e2e        the public C-ABI call cmd_run_batch with pinned host buffers
+             (initial state + pulses H2D, every step's observables D2H);
+  plain_path the plain per-trajectory path (one trajectory per launch,
+             random unit spins seed 1, 10^4 steps, observables every step);
+  cpu_baseline the oracle (CPU restatement of the reference integrator) on
+             a bounded sample of the same scan, all host threads.
+`--impl reference` times only the reference CPU path (the oracle port; the
+reference's own CPU build needs Eigen3/Boost/HDF5/MPI, absent here).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "batched LL spin\u00b7RK-steps/s on 1 B200 vs plain path; adjoint/forward cost"
+UNIT = "spin\u00b7RK-steps/s"
+FLOPS_PER_SPIN_STEP = 339.0        # 4*(18z + 9 + 12) + 39 with z = 3, drive on, no static field
+N_DELAYS = 256
+L_SIDE = 24
+
+
+# --------------------------------------------------------------------------- workload
+def scan_workload(n_steps: int, rank: int = 0, world: int = 1):
+    from classical_mcmc_spin_b200.lattice import Lattice
+    from classical_mcmc_spin_b200.states import zigzag_honeycomb
+
+    lat = Lattice.kitaev(L_SIDE, L_SIDE, 1, K=-1.0, Gamma=0.25, Gammap=-0.02)
+    s0 = zigzag_honeycomb(L_SIDE, L_SIDE, 1, tilt_sigma=0.05, seed=2).ravel()
+    fin = np.tile(np.ones(3) / np.sqrt(3.0), 2)
+    fd = lat.rotate_pulse(fin, fin)
+    # weak scaling: rank r scans the delays shifted by r/world of one delay step
+    taus = 100.0 * (np.arange(N_DELAYS) + rank / world) / (N_DELAYS - 1)
+    pulses = []
+    for tau in taus:
+        for a1, a2 in ((0.5, 0.0), (0.0, 0.5), (0.5, 0.5)):
+            pulses.append((0.0, tau, a1, a2))
+    pulses = np.array(pulses)
+    return dict(lat=lat, s0=s0, fin=fin, d1=fd[:6].copy(), d2=fd[6:].copy(), pulses=pulses, T0=-5.0, dt=0.01,
+                n_steps=n_steps, width=0.5, freq=0.0)
+
+
+# --------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.lines = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------- peaks
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return json.loads(p.read_text())
+    except Exception:
+        return {}
+
+
+def fp64_peak_tflops(torch) -> float:
+    """Dense FP64 peak measured here with cuBLAS DGEMM (best of 5, 8192^3)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+def profile_traffic():
+    """DRAM bytes per launch from the committed ncu summary, if present."""
+    p = ROOT / "profiles" / "rk4_resident_2dcs_kitaev1152.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# --------------------------------------------------------------------------- CPU baseline
+def cpu_baseline(wl, target_s: float = 8.0):
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import ll_oracle as O
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    lat = O.OracleLattice.kitaev(L_SIDE, L_SIDE, 1, K=-1.0, Gamma=0.25, Gammap=-0.02)
+    N = lat.N
+    P = wl["pulses"]
+    pick = np.linspace(0, len(P) - 1, max(threads, 8)).astype(int)
+    B = len(pick)
+    s = np.tile(wl["s0"], (B, 1))
+    sub = P[pick]
+    s1 = sub[:, 2] / 0.5
+    s2 = sub[:, 3] / 0.5
+
+    def run(steps):
+        t0 = time.perf_counter()
+        lat.batch_rk4(s, sub[:, 0], sub[:, 1], s1, s2, 0.5, wl["width"], wl["freq"], wl["fin"], wl["fin"], wl["T0"],
+                      wl["dt"], steps, with_obs=True, with_energy=False)
+        return time.perf_counter() - t0
+
+    probe = 20
+    tp = run(probe)
+    steps = int(max(20, min(20000, probe * target_s / max(tp, 1e-6))))
+    wall = run(steps)
+    return dict(value=B * N * steps / wall, unit=UNIT, cores=threads, kind="port",
+                sample=f"{B} of the 768 scan trajectories x {steps} RK4 steps (1152 spins, observables every step), "
+                       f"oracle restatement of the reference CPU RHS + RK4, trajectory-parallel OpenMP, "
+                       f"{wall:.2f} s wall"), (B, steps, wall)
+
+
+# --------------------------------------------------------------------------- reference arm
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    wl = scan_workload(args.md_steps)
+    results = []
+    for i in range(args.warmup + args.steps):
+        base, (B, steps, wall) = cpu_baseline(wl, target_s=args.cpu_seconds)
+        if i >= args.warmup:
+            results.append((base["value"], wall, B, steps))
+    vals = [r[0] for r in results]
+    v = statistics.median(vals)
+    B, steps = results[-1][2], results[-1][3]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * statistics.median([r[1] for r in results]), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "2dcs_scan_kitaev24x24_768traj_rk4", "sample_trajectories": B,
+                       "sample_steps": steps, "spins": L_SIDE * L_SIDE * 2},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                             "sample": f"{B} scan trajectories x {steps} RK4 steps per bench step; the reference's "
+                                       "own CPU build needs Eigen3/Boost/HDF5/MPI (absent), so the oracle "
+                                       "restatement of its CPU integrator is timed"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------- B200 arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--md-steps", type=int, default=20000, help="RK4 steps per trajectory (config: 2e4)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=8.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    from classical_mcmc_spin_b200 import _native as nat
+    from classical_mcmc_spin_b200 import gpu_api
+
+    wl = scan_workload(args.md_steps, rank, world)
+    lat = wl["lat"]
+    N = lat.lattice_size
+    P = wl["pulses"]
+    B = len(P)
+    S = wl["n_steps"]
+    h = lat.to_gpu()
+    rows = int(nat.lib().cmd_batch_rows(S, 1))
+    dev = torch.device("cuda", local)
+    d_states = torch.from_numpy(wl["s0"]).to(dev).contiguous()
+    d_pulse = torch.from_numpy(P.astype(np.float64)).to(dev).contiguous()
+    d_obs = torch.empty((B, rows, 10), dtype=torch.float64, device=dev)
+    d_fin = torch.empty((B, 3 * N), dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # > 126 MB L2
+    keep = dict(d1=wl["d1"], d2=wl["d2"])
+    desc = nat.BatchDesc()
+    desc.B = B
+    desc.states = d_states.data_ptr()
+    desc.shared_initial = 1
+    desc.method = nat.CMD_RK4
+    desc.d1 = keep["d1"].ctypes.data
+    desc.d2 = keep["d2"].ctypes.data
+    desc.width = wl["width"]
+    desc.freq = wl["freq"]
+    desc.T0 = wl["T0"]
+    desc.dt = wl["dt"]
+    desc.n_steps = S
+    desc.save_interval = 1
+    desc.obs = d_obs.data_ptr()
+    desc.final_states = d_fin.data_ptr()
+    desc.pulse4 = d_pulse.data_ptr()
+    launches = C.c_int32()
+
+    def launch():
+        st = torch.cuda.current_stream(dev).cuda_stream
+        nat.check(nat.lib().cmd_run_batch_device(h.ptr, C.byref(desc), C.c_void_p(st), C.byref(launches)),
+                  "cmd_run_batch_device")
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        launch()
+    torch.cuda.synchronize(dev)
+
+    sampler = ClockSampler(local)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    sampler.start()
+    time.sleep(0.3)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    n_launch = 0
+    t_start.record()
+    for k in range(args.steps):
+        flush.zero_()                       # L2 flush between timed iterations
+        ev[k][0].record()
+        launch()
+        ev[k][1].record()
+        n_launch += launches.value
+    t_end.record()
+    torch.cuda.synchronize(dev)
+    clocks = sampler.stop()
+    total_ms = t_start.elapsed_time(t_end)
+    kern_ms = [a.elapsed_time(b) for a, b in ev]
+    if dist is not None:
+        tt = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+        dist.barrier()
+    ms_per_step = total_ms / args.steps
+    value = world * B * N * S / (ms_per_step * 1e-3)
+    kernel_ms = statistics.mean(kern_ms)
+
+    # ---- parity spot check of the benched run against itself: finite, unit norm
+    obs_last = d_obs[:, -1, :].cpu().numpy()
+    fin = d_fin.view(B, N, 3)
+    norm_dev = float((fin.norm(dim=2) - 1).abs().max().item())
+    finite = bool(np.isfinite(obs_last).all())
+
+    # ---- end to end through the public C ABI (pinned host buffers)
+    e2e = None
+    if not args.no_e2e:
+        h_init = torch.from_numpy(wl["s0"]).pin_memory()
+        h_obs = torch.empty((B, rows, 10), dtype=torch.float64).pin_memory()
+        t1 = np.ascontiguousarray(P[:, 0]); t2 = np.ascontiguousarray(P[:, 1])
+        a1 = np.ascontiguousarray(P[:, 2]); a2 = np.ascontiguousarray(P[:, 3])
+        hd = nat.BatchDesc()
+        hd.B = B
+        hd.states = h_init.data_ptr()
+        hd.shared_initial = 1
+        hd.method = nat.CMD_RK4
+        hd.t1, hd.t2, hd.a1, hd.a2 = t1.ctypes.data, t2.ctypes.data, a1.ctypes.data, a2.ctypes.data
+        hd.d1 = keep["d1"].ctypes.data
+        hd.d2 = keep["d2"].ctypes.data
+        hd.width, hd.freq, hd.T0, hd.dt = wl["width"], wl["freq"], wl["T0"], wl["dt"]
+        hd.n_steps, hd.save_interval = S, 1
+        hd.obs = h_obs.data_ptr()
+        hd.final_states = None
+        nat.check(nat.lib().cmd_run_batch(h.ptr, C.byref(hd)), "cmd_run_batch")   # warm
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        n_e2e = max(1, min(args.steps, 3))
+        for _ in range(n_e2e):
+            nat.check(nat.lib().cmd_run_batch(h.ptr, C.byref(hd)), "cmd_run_batch")
+        torch.cuda.synchronize(dev)
+        e2e_s = (time.perf_counter() - t0) / n_e2e
+        if dist is not None:
+            tt = torch.tensor([e2e_s], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e2e_s = float(tt.item())
+        e2e = {"value": world * B * N * S / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(h_init.numel() * 8 + P.size * 8),
+               "d2h_bytes_per_step": int(h_obs.numel() * 8)}
+        del h_obs
+
+    # ---- plain path: one trajectory per launch (drop-in integrate_gpu)
+    plain = None
+    if not args.no_plain and rank == 0:
+        from classical_mcmc_spin_b200.states import random_unit_spins
+        s1 = random_unit_spins(N, 1).ravel()
+        gpu_api.set_gpu_spins(h, s1)
+        gpu_api.integrate_gpu(h, 0.0, 1.0, 0.01, 1, "rk4", with_states=False)     # warm
+        gpu_api.set_gpu_spins(h, s1)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        _, pobs, ptimes = gpu_api.integrate_gpu(h, 0.0, 99.995, 0.01, 1, "rk4", with_states=False)
+        dtp = time.perf_counter() - t0
+        nsteps = len(ptimes) - 1
+        plain = {"value": N * nsteps / dtp, "unit": UNIT, "steps": nsteps,
+                 "workload": "plain MD Kitaev 24x24 (1152 spins), random spins seed 1, RK4 dt=0.01, "
+                             "M and E every step, via integrate_gpu (host buffers)"}
+
+    peaks = measured_peaks()
+    fp64 = fp64_peak_tflops(torch) if rank == 0 else None
+    achieved_tflops = FLOPS_PER_SPIN_STEP * B * N * S / (kernel_ms * 1e-3) / 1e12
+    traffic = profile_traffic()
+    roofline = {"bound": "fp64", "achieved": achieved_tflops, "peak": fp64, "unit": "TFLOP/s",
+                "frac": (achieved_tflops / fp64) if fp64 else None, "traffic": traffic,
+                "peak_source": "measured in this run: cuBLAS DGEMM 8192^3 best of 5 (MEASURED_PEAKS.json "
+                               "has no FP64 figure; the kernel is FP64-pipe bound, not HBM or tensor)",
+                "flops_per_spin_step": FLOPS_PER_SPIN_STEP,
+                "kernel_ms_per_launch": kernel_ms,
+                "hbm_peak_gbs_measured": peaks.get("hbm_gbs")}
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu, _ = cpu_baseline(wl, target_s=args.cpu_seconds)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "2dcs_scan_kitaev24x24_768traj_rk4", "spins": N, "trajectories": B,
+                           "rk4_steps": S, "dt": wl["dt"], "T_start": wl["T0"], "delays": N_DELAYS,
+                           "observables_every_step": True, "l2": "flushed between timed iterations (256 MB write)",
+                           "parallelism": f"replicas: {world} GPU(s), trajectories sharded, no collective"},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+                "gpu_launches": n_launch, "plain_path": plain,
+                "batched_over_plain": (value / world) / plain["value"] if plain else None,
+                "adjoint_over_forward": None,
+                "checks": {"final_norm_dev_max": norm_dev, "observables_finite": finite}}
+        print(json.dumps(line), flush=True)
+    h.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

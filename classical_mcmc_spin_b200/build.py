@@ -1,0 +1,69 @@
+"""Build recipe for the native library of the B200 LL MD path.
+
+``python -m classical_mcmc_spin_b200.build`` compiles every CUDA/C++ source
+under ``csrc/`` for sm_100a into ``libcmd_b200.so`` next to this file (in the
+source tree, so the built library travels with the repository snapshot).
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+LIB = PKG / "libcmd_b200.so"
+BUILD = PKG / "_build"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "--expt-relaxed-constexpr",
+              "-Xcompiler", "-fPIC", "-Xcompiler", "-O3"]
+SOURCES = ["cmd_api.cu", "lattice_host.cpp"]
+
+
+def nvcc() -> str:
+    cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(cand).exists():
+        raise RuntimeError("nvcc not found; the CUDA toolkit is required to build libcmd_b200.so")
+    return cand
+
+
+def _newer(target: Path, deps) -> bool:
+    if not target.exists():
+        return False
+    t = target.stat().st_mtime
+    return all(Path(d).stat().st_mtime <= t for d in deps)
+
+
+def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) -> Path:
+    deps = [CSRC / s for s in SOURCES] + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) \
+        + list((ROOT / "include").glob("*.h"))
+    if not force and not ptxas_info and _newer(LIB, deps):
+        return LIB
+    BUILD.mkdir(exist_ok=True)
+    objs = []
+    inc = ["-I", str(ROOT / "include"), "-I", str(CSRC)]
+    for src in SOURCES:
+        obj = BUILD / (Path(src).stem + ".o")
+        cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *inc, "-c", str(CSRC / src), "-o", str(obj)]
+        if ptxas_info and src.endswith(".cu"):
+            cmd.insert(1, "-Xptxas=-v")
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+        objs.append(str(obj))
+    tmp = LIB.with_suffix(".so.tmp")
+    cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose=True, force="--force" in sys.argv, ptxas_info="--ptxas" in sys.argv)
+    print(LIB)

@@ -1,0 +1,815 @@
+// cmd_api.cu -- C-ABI implementation of the B200 Landau-Lifshitz MD path.
+//
+// Replaces the reference's gpu:: host API (include/classical_spin/gpu/
+// lattice_gpu_api.h; implementation src/gpu/lattice_gpu.cu:586-791).  The
+// reference keeps the lattice as an ELL table of per-entry 3x3 matrices and
+// runs each RK stage as separate kernel launches with a device-wide sync in
+// between (integrator.cuh:115-139: 8 launches + 4 syncs per step).  Here the
+// lattice is compiled once at cmd_create into a per-unit-cell coupling table
+// (identical for every cell, so it lives in kernel parameters) plus int32
+// neighbour offsets, and a whole trajectory -- every stage of every step and
+// the per-step observables -- runs inside one CTA of one launch.
+#include "cmd.h"
+#include "cmd_internal.h"
+#include "rk4_resident.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace cmd {
+
+static thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+void clear_error() { g_last_error.clear(); }
+
+}  // namespace cmd
+
+using cmd::fail;
+
+namespace {
+
+constexpr size_t kMaxSmem = 232448;   // 227 KB dynamic shared memory per CTA on sm_100
+
+#define CUDA_TRY(expr)                                                                   \
+    do {                                                                                 \
+        cudaError_t e_ = (expr);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return fail(e_ == cudaErrorMemoryAllocation ? CMD_ERR_OOM : CMD_ERR_CUDA,    \
+                        std::string(#expr) + ": " + cudaGetErrorString(e_));             \
+    } while (0)
+
+// Per-unit-cell description of the lattice, derived from the flat tables.
+struct Layout {
+    int NA = 0;                 // sites per cell (= classes)
+    int64_t G = 0;              // cells
+    int Z = 0;                  // slots per atom (max over atoms)
+    int LZ = 0;                 // leading "local" slots (partner in the same cell)
+    std::vector<int> zc;        // slots per atom
+    std::vector<double> J;      // [NA][Z][9]
+    std::vector<int> nbr;       // [G][NA][Z-LZ] shared-memory offsets
+    bool uniform = false;
+    std::string why;            // reason when not uniform
+};
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t n) {
+        if (n <= bytes) return CMD_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return fail(CMD_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        }
+        bytes = n;
+        return CMD_OK;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+}  // namespace
+
+struct cmd_handle {
+    int64_t N = 0;
+    int NA = 0;
+    int zmax = 0;
+    std::vector<double> field, onsite, frames, afm;   // field/onsite per site; frames/afm per atom
+    bool has_field = false, has_onsite = false;
+    Layout lay;
+    cudaStream_t stream = nullptr;
+    DevBuf state, nbr, obs, traj, batch_states, batch_out, pulses, scratch;
+    bool has_state = false;
+    // pulse (set_gpu_pulse)
+    std::vector<double> fd;     // [2][NA*3]
+    double amp = 0.0, width = 1.0, freq = 0.0, t1 = 0.0, t2 = 0.0;
+    // controlled stepper
+    double abs_tol = 1e-6, rel_tol = 1e-6;
+    int64_t max_steps = 0;
+};
+
+namespace {
+
+bool mat_equal(const double* a, const double* b) { return std::memcmp(a, b, 9 * sizeof(double)) == 0; }
+bool mat_zero(const double* a) {
+    for (int i = 0; i < 9; ++i)
+        if (a[i] != 0.0) return false;
+    return true;
+}
+
+// Compile the flat ELL tables into the per-cell layout.  Requirements (every
+// lattice the reference builds from a UnitCell satisfies them): N = NA * G,
+// field/onsite depend on the atom only, and after dropping all-zero coupling
+// entries (which add exactly 0.0) each site of atom a carries the same
+// multiset of (J, partner atom) as the site of atom a in cell 0.
+void analyse(const cmd_lattice_desc& d, Layout& L) {
+    L = Layout{};
+    const int64_t N = d.lattice_size;
+    const int NA = d.n_atoms;
+    const int zmax = d.max_bilinear;
+    if (NA <= 0 || N % NA != 0) { L.why = "lattice_size is not a multiple of n_atoms"; return; }
+    L.NA = NA;
+    L.G = N / NA;
+    for (int64_t i = 0; i < N; ++i) {
+        const int a = (int)(i % NA);
+        if (std::memcmp(&d.field[3 * i], &d.field[3 * a], 3 * sizeof(double)) != 0 ||
+            std::memcmp(&d.onsite[9 * i], &d.onsite[9 * a], 9 * sizeof(double)) != 0) {
+            L.why = "field or onsite term differs between cells";
+            return;
+        }
+    }
+    // canonical (cell 0) slot lists per atom
+    struct Slot { const double* J; int b; int64_t p0; };   // p0: partner seen from cell 0
+    std::vector<std::vector<Slot>> canon(NA);
+    for (int a = 0; a < NA; ++a) {
+        for (int64_t n = 0; n < d.counts[a]; ++n) {
+            const double* J = &d.bilinear[9 * (a * (int64_t)zmax + n)];
+            if (mat_zero(J)) continue;
+            const int64_t p = d.partners[a * (int64_t)zmax + n];
+            canon[a].push_back(Slot{J, (int)(p % NA), p});
+        }
+    }
+    // Try local-first ordering: slot n < NA-1 of atom a bonds to atom (a+1+n)%NA
+    // inside the same cell.
+    auto attempt = [&](bool local_first) -> bool {
+        int LZ = 0;
+        std::vector<std::vector<Slot>> order(NA);
+        if (local_first) {
+            LZ = NA - 1;
+            for (int a = 0; a < NA; ++a) {
+                std::vector<char> used(canon[a].size(), 0);
+                for (int n = 0; n < NA - 1; ++n) {
+                    const int want = (a + 1 + n) % NA;
+                    int pick = -1;
+                    for (size_t q = 0; q < canon[a].size(); ++q) {
+                        if (used[q] || canon[a][q].b != want) continue;
+                        if (canon[a][q].p0 / NA != 0) continue;   // must stay inside cell 0
+                        pick = (int)q;
+                        break;
+                    }
+                    if (pick < 0) return false;
+                    used[pick] = 1;
+                    order[a].push_back(canon[a][pick]);
+                }
+                for (size_t q = 0; q < canon[a].size(); ++q)
+                    if (!used[q]) order[a].push_back(canon[a][q]);
+            }
+        } else {
+            order = canon;
+        }
+        int Z = 0;
+        for (int a = 0; a < NA; ++a) Z = std::max(Z, (int)order[a].size());
+        const int NL = Z - LZ;
+        const int64_t G = L.G;
+        std::vector<int> nbr((size_t)G * NA * std::max(NL, 1), 0);
+        std::vector<char> taken(zmax);
+        for (int64_t g = 0; g < G; ++g) {
+            for (int a = 0; a < NA; ++a) {
+                const int64_t i = g * NA + a;
+                std::fill(taken.begin(), taken.end(), 0);
+                const int64_t cnt = d.counts[i];
+                int nz = 0;
+                for (int64_t n = 0; n < cnt; ++n)
+                    if (!mat_zero(&d.bilinear[9 * (i * zmax + n)])) ++nz;
+                if (nz != (int)order[a].size()) return false;
+                for (int s = 0; s < (int)order[a].size(); ++s) {
+                    const Slot& sl = order[a][s];
+                    int pick = -1;
+                    for (int64_t n = 0; n < cnt; ++n) {
+                        if (taken[n]) continue;
+                        const int64_t p = d.partners[i * zmax + n];
+                        if (p < 0 || p >= d.lattice_size) return false;
+                        if ((int)(p % NA) != sl.b) continue;
+                        if (!mat_equal(&d.bilinear[9 * (i * zmax + n)], sl.J)) continue;
+                        if (s < LZ && p / NA != g) continue;   // local slot: same cell
+                        pick = (int)n;
+                        break;
+                    }
+                    if (pick < 0) return false;
+                    taken[pick] = 1;
+                    if (s >= LZ) {
+                        const int64_t p = d.partners[i * zmax + pick];
+                        const int64_t off = (int64_t)(p % NA) * 3 * G + p / NA;
+                        if (off > INT32_MAX) return false;
+                        nbr[((size_t)g * NA + a) * NL + (s - LZ)] = (int)off;
+                    }
+                }
+            }
+        }
+        L.LZ = LZ;
+        L.Z = Z;
+        L.zc.resize(NA);
+        L.J.assign((size_t)NA * std::max(Z, 1) * 9, 0.0);
+        for (int a = 0; a < NA; ++a) {
+            L.zc[a] = (int)order[a].size();
+            for (int s = 0; s < (int)order[a].size(); ++s)
+                std::memcpy(&L.J[((size_t)a * Z + s) * 9], order[a][s].J, 9 * sizeof(double));
+        }
+        L.nbr.swap(nbr);
+        return true;
+    };
+    if (attempt(true) || attempt(false)) {
+        L.uniform = true;
+        return;
+    }
+    L.why = "coupling table is not identical in every unit cell";
+}
+
+template <int NAT, int Z>
+void fill_couplings(const cmd_handle* h, const double* frames, const double* afm, const double* d1,
+                    const double* d2, cmd::Couplings<NAT, Z>& cp) {
+    std::memset(&cp, 0, sizeof(cp));
+    const Layout& L = h->lay;
+    for (int a = 0; a < NAT; ++a) {
+        for (int s = 0; s < Z && s < L.zc[a]; ++s)
+            std::memcpy(cp.J[a][s], &L.J[((size_t)a * L.Z + s) * 9], 9 * sizeof(double));
+        cp.zc[a] = L.zc[a];
+        std::memcpy(cp.field[a], &h->field[3 * a], 3 * sizeof(double));
+        std::memcpy(cp.onsite[a], &h->onsite[9 * a], 9 * sizeof(double));
+        std::memcpy(cp.frame[a], (frames ? frames : h->frames.data()) + 9 * a, 9 * sizeof(double));
+        cp.afm[a] = (afm ? afm : h->afm.data())[a];
+        if (d1) std::memcpy(cp.d1[a], d1 + 3 * a, 3 * sizeof(double));
+        if (d2) std::memcpy(cp.d2[a], d2 + 3 * a, 3 * sizeof(double));
+    }
+    cp.has_field = h->has_field;
+    cp.has_onsite = h->has_onsite;
+}
+
+struct ResidentPlan {
+    int threads = 0, cpt = 0;
+    size_t smem = 0;
+};
+
+size_t resident_smem(int NA, int64_t G) {
+    return (size_t)2 * NA * 3 * G * sizeof(double) + (32 * cmd::kRedStride + 16 + 12) * sizeof(double);
+}
+
+template <int NAT, int Z, int LZ, int CPT, int MAXT>
+int launch_one(const cmd_handle* h, const cmd::ResidentArgs& args, const double* frames,
+               const double* afm, const double* d1, const double* d2, int64_t B,
+               cudaStream_t st, ResidentPlan* plan) {
+    auto kern = cmd::rk4_resident_kernel<NAT, Z, LZ, CPT, MAXT>;
+    const int64_t G = h->lay.G;
+    int threads = (int)((G + CPT - 1) / CPT);
+    threads = ((threads + 31) / 32) * 32;
+    if (threads > MAXT) return fail(CMD_ERR_UNSUPPORTED, "lattice too large for the resident kernel");
+    const size_t smem = resident_smem(NAT, G);
+    if (smem > kMaxSmem) return fail(CMD_ERR_UNSUPPORTED, "stage buffers exceed shared memory");
+    static bool attr_set = false;
+    if (!attr_set) {
+        CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
+        attr_set = true;
+    }
+    if (plan) { plan->threads = threads; plan->cpt = CPT; plan->smem = smem; }
+    if (B <= 0) return CMD_OK;      // plan only
+    cmd::Couplings<NAT, Z> cp;
+    fill_couplings<NAT, Z>(h, frames, afm, d1, d2, cp);
+    kern<<<(unsigned)B, threads, smem, st>>>(cp, args);
+    CUDA_TRY(cudaGetLastError());
+    return CMD_OK;
+}
+
+// Resident-kernel instances compiled into the library.
+enum Instance { kNone = 0, kHoney1, kHoney2, kPyro1, kPyro2 };
+
+Instance pick_instance(const Layout& L) {
+    if (!L.uniform) return kNone;
+    if (L.NA == 2 && L.Z == 3 && L.LZ == 1) {
+        if (L.G <= 640) return kHoney1;
+        if (L.G <= 1024) return kHoney2;
+    } else if (L.NA == 4 && L.Z == 6 && L.LZ == 3) {
+        if (L.G <= 512) return kPyro1;
+        if (L.G <= 1024) return kPyro2;
+    }
+    return kNone;
+}
+
+int instance_cpt(Instance i) { return (i == kHoney2 || i == kPyro2) ? 2 : (i == kNone ? 0 : 1); }
+
+int no_instance(const Layout& L) {
+    if (!L.uniform) return fail(CMD_ERR_UNSUPPORTED, "lattice layout not supported: " + L.why);
+    char buf[200];
+    std::snprintf(buf, sizeof(buf),
+                  "no resident kernel for %d atoms/cell, %d bonds/site, %d local, %lld cells",
+                  L.NA, L.Z, L.LZ, (long long)L.G);
+    return fail(CMD_ERR_UNSUPPORTED, buf);
+}
+
+// Launches the kernel instance for the handle's layout; B = 0 only fills `plan`.
+int launch_resident(const cmd_handle* h, const cmd::ResidentArgs& args, const double* frames,
+                    const double* afm, const double* d1, const double* d2, int64_t B,
+                    cudaStream_t st, ResidentPlan* plan = nullptr) {
+    switch (pick_instance(h->lay)) {
+        case kHoney1: return launch_one<2, 3, 1, 1, 640>(h, args, frames, afm, d1, d2, B, st, plan);
+        case kHoney2: return launch_one<2, 3, 1, 2, 512>(h, args, frames, afm, d1, d2, B, st, plan);
+        case kPyro1: return launch_one<4, 6, 3, 1, 512>(h, args, frames, afm, d1, d2, B, st, plan);
+        case kPyro2: return launch_one<4, 6, 3, 2, 512>(h, args, frames, afm, d1, d2, B, st, plan);
+        default: return no_instance(h->lay);
+    }
+}
+
+int64_t rows_for(int64_t n_steps, int64_t save) { return (n_steps + save - 1) / save + 1; }
+
+// Reference GPU loop (integrator.cuh:477-483): number of steps and times.
+int64_t count_steps(double T0, double T1, double dt, double margin, std::vector<double>* times) {
+    int64_t n = 0;
+    double t = T0;
+    while (t < T1 - margin) {
+        if (times) times->push_back(t);
+        t += dt;
+        ++n;
+        if (n > (int64_t)1 << 40) break;
+    }
+    if (times) times->push_back(t);
+    return n;
+}
+
+int sync(cmd_handle* h) {
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return fail(CMD_ERR_CUDA, std::string("kernel execution: ") + cudaGetErrorString(e));
+    return CMD_OK;
+}
+
+__global__ void normalize_kernel(double* s, double len, int64_t N) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const double x = s[3 * i], y = s[3 * i + 1], z = s[3 * i + 2];
+    const double n = sqrt(x * x + y * y + z * z);
+    if (n > 0.0) {
+        s[3 * i] = len * x / n;
+        s[3 * i + 1] = len * y / n;
+        s[3 * i + 2] = len * z / n;
+    }
+}
+
+// compute_magnetization_gpu semantics: mean and (-1)^i staggered mean.  One CTA,
+// fixed-order tree reduction.
+__global__ void magnetization_kernel(const double* s, int64_t N, double* out) {
+    __shared__ double sh[6][256];
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    for (int64_t i = threadIdx.x; i < N; i += blockDim.x) {
+        const double sg = (i % 2 == 0) ? 1.0 : -1.0;
+        for (int c = 0; c < 3; ++c) {
+            v[c] += s[3 * i + c];
+            v[3 + c] += sg * s[3 * i + c];
+        }
+    }
+    for (int q = 0; q < 6; ++q) sh[q][threadIdx.x] = v[q];
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int q = 0; q < 6; ++q) sh[q][threadIdx.x] += sh[q][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 6; ++q) out[q] = sh[q][0] / (double)N;
+}
+
+int check_handle(cmd_handle* h, bool need_state) {
+    if (!h) return fail(CMD_ERR_INVALID_ARG, "NULL handle");
+    if (need_state && !h->has_state) return fail(CMD_ERR_STATE, "spins not set (call cmd_set_spins first)");
+    return CMD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cmd_last_error(void) { return cmd::g_last_error.c_str(); }
+const char* cmd_version(void) { return "classical_mcmc_spin_b200 0.1 (sm_100a, fp64)"; }
+
+int cmd_create(const cmd_lattice_desc* d, cmd_handle** out) {
+    cmd::clear_error();
+    if (!out) return fail(CMD_ERR_INVALID_ARG, "output pointer is NULL");
+    *out = nullptr;
+    if (!d) return fail(CMD_ERR_INVALID_ARG, "NULL lattice description");
+    if (d->spin_dim != 3) return fail(CMD_ERR_UNSUPPORTED, "only spin_dim = 3 is supported");
+    if (d->lattice_size <= 0 || d->n_atoms <= 0 || d->max_bilinear < 0)
+        return fail(CMD_ERR_INVALID_ARG, "bad lattice sizes");
+    if (d->lattice_size > ((int64_t)1 << 30)) return fail(CMD_ERR_INVALID_ARG, "lattice too large");
+    if (!d->field || !d->onsite || !d->counts || (d->max_bilinear > 0 && (!d->bilinear || !d->partners)))
+        return fail(CMD_ERR_INVALID_ARG, "NULL lattice array");
+    for (int64_t i = 0; i < d->lattice_size; ++i)
+        if (d->counts[i] < 0 || d->counts[i] > d->max_bilinear)
+            return fail(CMD_ERR_INVALID_ARG, "bilinear count out of range");
+    for (int64_t i = 0; i < d->lattice_size * 3; ++i)
+        if (!std::isfinite(d->field[i])) return fail(CMD_ERR_NONFINITE, "non-finite field");
+    for (int64_t i = 0; i < d->lattice_size * d->max_bilinear * 9; ++i)
+        if (!std::isfinite(d->bilinear[i])) return fail(CMD_ERR_NONFINITE, "non-finite coupling");
+    cmd_handle* h = new (std::nothrow) cmd_handle();
+    if (!h) return fail(CMD_ERR_OOM, "host allocation failed");
+    h->N = d->lattice_size;
+    h->NA = d->n_atoms;
+    h->zmax = d->max_bilinear;
+    h->field.assign(d->field, d->field + 3 * d->n_atoms);
+    h->onsite.assign(d->onsite, d->onsite + 9 * d->n_atoms);
+    h->frames.assign(9 * (size_t)d->n_atoms, 0.0);
+    h->afm.assign(d->n_atoms, 1.0);
+    for (int a = 0; a < d->n_atoms; ++a) {
+        if (d->frames) std::memcpy(&h->frames[9 * a], d->frames + 9 * a, 9 * sizeof(double));
+        else h->frames[9 * a] = h->frames[9 * a + 4] = h->frames[9 * a + 8] = 1.0;
+        if (d->afm_signs) h->afm[a] = d->afm_signs[a];
+    }
+    for (double v : h->field) h->has_field |= (v != 0.0);
+    for (double v : h->onsite) h->has_onsite |= (v != 0.0);
+    h->fd.assign(2 * 3 * (size_t)d->n_atoms, 0.0);
+    analyse(*d, h->lay);
+    int rc = CMD_OK;
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        rc = fail(CMD_ERR_CUDA, "cudaStreamCreate failed (no CUDA device?)");
+    } else if (h->lay.uniform) {
+        rc = h->nbr.ensure(std::max<size_t>(h->lay.nbr.size(), 1) * sizeof(int));
+        if (rc == CMD_OK && !h->lay.nbr.empty() &&
+            cudaMemcpy(h->nbr.p, h->lay.nbr.data(), h->lay.nbr.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+            rc = fail(CMD_ERR_CUDA, "neighbour table upload failed");
+    }
+    if (rc == CMD_OK) rc = h->state.ensure((size_t)h->N * 3 * sizeof(double));
+    if (rc != CMD_OK) {
+        cmd_destroy(h);
+        return rc;
+    }
+    *out = h;
+    return CMD_OK;
+}
+
+int cmd_destroy(cmd_handle* h) {
+    if (!h) return CMD_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (DevBuf* b : {&h->state, &h->nbr, &h->obs, &h->traj, &h->batch_states, &h->batch_out,
+                      &h->pulses, &h->scratch})
+        b->release();
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return CMD_OK;
+}
+
+int cmd_set_pulse(cmd_handle* h, const double* fd, double amp, double width, double freq, double t1,
+                  double t2) {
+    cmd::clear_error();
+    if (int rc = check_handle(h, false)) return rc;
+    if (!fd) return fail(CMD_ERR_INVALID_ARG, "NULL field_drive");
+    if (!(width != 0.0) || !std::isfinite(amp) || !std::isfinite(width) || !std::isfinite(freq))
+        return fail(CMD_ERR_INVALID_ARG, "bad pulse parameters");
+    h->fd.assign(fd, fd + 6 * (size_t)h->NA);
+    h->amp = amp; h->width = width; h->freq = freq; h->t1 = t1; h->t2 = t2;
+    return CMD_OK;
+}
+
+int cmd_set_spins(cmd_handle* h, const double* s, int64_t n) {
+    cmd::clear_error();
+    if (int rc = check_handle(h, false)) return rc;
+    if (!s || n != h->N * 3) return fail(CMD_ERR_INVALID_ARG, "spin array must hold N*3 doubles");
+    for (int64_t i = 0; i < n; ++i)
+        if (!std::isfinite(s[i])) return fail(CMD_ERR_NONFINITE, "non-finite spin component");
+    CUDA_TRY(cudaMemcpyAsync(h->state.p, s, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    if (int rc = sync(h)) return rc;
+    h->has_state = true;
+    return CMD_OK;
+}
+
+int cmd_get_spins(cmd_handle* h, double* s, int64_t n) {
+    cmd::clear_error();
+    if (int rc = check_handle(h, true)) return rc;
+    if (!s || n != h->N * 3) return fail(CMD_ERR_INVALID_ARG, "spin array must hold N*3 doubles");
+    CUDA_TRY(cudaMemcpyAsync(s, h->state.p, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    return sync(h);
+}
+
+int cmd_set_tolerances(cmd_handle* h, double abs_tol, double rel_tol, int64_t max_steps) {
+    cmd::clear_error();
+    if (int rc = check_handle(h, false)) return rc;
+    if (!(abs_tol >= 0.0) || !(rel_tol >= 0.0) || (abs_tol == 0.0 && rel_tol == 0.0) || max_steps < 0)
+        return fail(CMD_ERR_INVALID_ARG, "bad tolerances");
+    h->abs_tol = abs_tol; h->rel_tol = rel_tol; h->max_steps = max_steps;
+    return CMD_OK;
+}
+
+namespace {
+
+// Runs `n_steps` RK4 steps of the handle's trajectory on device, saving rows.
+int run_single(cmd_handle* h, double T0, double dt, int64_t n_steps, int64_t save, double n_sites,
+               bool want_obs, bool want_traj, bool with_pulse) {
+    const int64_t rows = rows_for(n_steps, save);
+    if (want_obs)
+        if (int rc = h->obs.ensure((size_t)rows * 10 * sizeof(double))) return rc;
+    if (want_traj)
+        if (int rc = h->traj.ensure((size_t)rows * h->N * 3 * sizeof(double))) return rc;
+    cmd::Pulse pl{h->t1, h->t2, h->amp, h->amp};
+    if (with_pulse && h->amp != 0.0) {
+        if (int rc = h->pulses.ensure(sizeof(cmd::Pulse))) return rc;
+        CUDA_TRY(cudaMemcpyAsync(h->pulses.p, &pl, sizeof(pl), cudaMemcpyHostToDevice, h->stream));
+    }
+    cmd::ResidentArgs a{};
+    a.G = (int)h->lay.G;
+    a.nonlocal = h->lay.Z - h->lay.LZ;
+    a.n_steps = n_steps;
+    a.save_every = save;
+    a.T0 = T0;
+    a.dt = dt;
+    a.n_sites = n_sites;
+    a.nbr = h->nbr.as<int>();
+    a.y0 = h->state.as<double>();
+    a.y0_stride = 0;
+    a.y_out = h->state.as<double>();
+    a.obs = want_obs ? h->obs.as<double>() : nullptr;
+    a.rows = rows;
+    a.traj = want_traj ? h->traj.as<double>() : nullptr;
+    a.pulses = (with_pulse && h->amp != 0.0) ? h->pulses.as<cmd::Pulse>() : nullptr;
+    a.width = h->width;
+    a.freq = h->freq;
+    const double* d1 = h->fd.data();
+    const double* d2 = h->fd.data() + 3 * h->NA;
+    if (int rc = launch_resident(h, a, nullptr, nullptr, d1, d2, 1, h->stream)) return rc;
+    return sync(h);
+}
+
+}  // namespace
+
+int cmd_step(cmd_handle* h, double t, double dt, int method) {
+    cmd::clear_error();
+    if (int rc = check_handle(h, true)) return rc;
+    if (method != CMD_RK4) return fail(CMD_ERR_UNSUPPORTED, "cmd_step: only CMD_RK4 is implemented");
+    if (!std::isfinite(t) || !std::isfinite(dt)) return fail(CMD_ERR_INVALID_ARG, "non-finite t or dt");
+    return run_single(h, t, dt, 1, 1, (double)h->N, false, false, true);
+}
+
+int cmd_integrate(cmd_handle* h, double T0, double T1, double dt, int64_t save_interval, int method,
+                  double* times, double* obs, double* states, int64_t max_rows, int64_t* rows_out) {
+    cmd::clear_error();
+    if (int rc = check_handle(h, true)) return rc;
+    if (method != CMD_RK4) return fail(CMD_ERR_UNSUPPORTED, "cmd_integrate: only CMD_RK4 is implemented");
+    if (save_interval <= 0 || !(dt > 0.0) || !std::isfinite(T0) || !std::isfinite(T1))
+        return fail(CMD_ERR_INVALID_ARG, "bad integration window");
+    std::vector<double> grid;
+    const int64_t n = count_steps(T0, T1, dt, 0.0, &grid);
+    const int64_t rows = rows_for(n, save_interval);
+    if (rows_out) *rows_out = rows;
+    if (max_rows < rows) return fail(CMD_ERR_INVALID_ARG, "max_rows too small");
+    if (int rc = run_single(h, T0, dt, n, save_interval, (double)h->N, obs != nullptr, states != nullptr, true))
+        return rc;
+    if (times) {
+        int64_t r = 0;
+        for (int64_t k = 0; k < n; k += save_interval) times[r++] = grid[k];
+        times[r] = grid[n];
+    }
+    if (obs) CUDA_TRY(cudaMemcpy(obs, h->obs.p, rows * 10 * sizeof(double), cudaMemcpyDeviceToHost));
+    if (states)
+        CUDA_TRY(cudaMemcpy(states, h->traj.p, rows * h->N * 3 * sizeof(double), cudaMemcpyDeviceToHost));
+    return CMD_OK;
+}
+
+int cmd_observables(cmd_handle* h, double* row) {
+    cmd::clear_error();
+    if (int rc = check_handle(h, true)) return rc;
+    if (!row) return fail(CMD_ERR_INVALID_ARG, "NULL row");
+    if (int rc = run_single(h, 0.0, 0.0, 0, 1, (double)h->N, true, false, false)) return rc;
+    CUDA_TRY(cudaMemcpy(row, h->obs.p, 10 * sizeof(double), cudaMemcpyDeviceToHost));
+    return CMD_OK;
+}
+
+int cmd_energy(cmd_handle* h, double* energy) {
+    cmd::clear_error();
+    if (int rc = check_handle(h, true)) return rc;
+    if (!energy) return fail(CMD_ERR_INVALID_ARG, "NULL energy");
+    if (int rc = run_single(h, 0.0, 0.0, 0, 1, 1.0, true, false, false)) return rc;
+    double row[10];
+    CUDA_TRY(cudaMemcpy(row, h->obs.p, sizeof(row), cudaMemcpyDeviceToHost));
+    *energy = row[9];
+    return CMD_OK;
+}
+
+int cmd_normalize(cmd_handle* h, double spin_length) {
+    cmd::clear_error();
+    if (int rc = check_handle(h, true)) return rc;
+    if (!std::isfinite(spin_length)) return fail(CMD_ERR_INVALID_ARG, "bad spin length");
+    const int64_t N = h->N;
+    normalize_kernel<<<(unsigned)((N + 255) / 256), 256, 0, h->stream>>>(h->state.as<double>(), spin_length, N);
+    CUDA_TRY(cudaGetLastError());
+    return sync(h);
+}
+
+int cmd_magnetization(cmd_handle* h, double* ml, double* ms) {
+    cmd::clear_error();
+    if (int rc = check_handle(h, true)) return rc;
+    if (!ml || !ms) return fail(CMD_ERR_INVALID_ARG, "NULL output");
+    if (int rc = h->scratch.ensure(6 * sizeof(double))) return rc;
+    magnetization_kernel<<<1, 256, 0, h->stream>>>(h->state.as<double>(), h->N, h->scratch.as<double>());
+    CUDA_TRY(cudaGetLastError());
+    if (int rc = sync(h)) return rc;
+    double v[6];
+    CUDA_TRY(cudaMemcpy(v, h->scratch.p, sizeof(v), cudaMemcpyDeviceToHost));
+    std::memcpy(ml, v, 3 * sizeof(double));
+    std::memcpy(ms, v + 3, 3 * sizeof(double));
+    return CMD_OK;
+}
+
+int64_t cmd_batch_rows(int64_t n_steps, int64_t save_interval) {
+    if (n_steps < 0 || save_interval <= 0) return -1;
+    return rows_for(n_steps, save_interval);
+}
+
+namespace {
+
+int validate_batch(const cmd_handle* h, const cmd_batch_desc* d) {
+    if (!d) return fail(CMD_ERR_INVALID_ARG, "NULL batch description");
+    if (d->B <= 0 || d->B > (1 << 24)) return fail(CMD_ERR_INVALID_ARG, "bad batch size");
+    if (d->method != CMD_RK4) return fail(CMD_ERR_UNSUPPORTED, "batched path implements CMD_RK4 only");
+    if (!d->states || !d->obs) return fail(CMD_ERR_INVALID_ARG, "NULL states or obs");
+    if (d->n_steps < 0 || d->save_interval <= 0 || !(d->dt > 0.0) || !std::isfinite(d->T0))
+        return fail(CMD_ERR_INVALID_ARG, "bad time grid");
+    const bool drive = d->d1 || d->d2;
+    if (drive && !d->pulse4 && (!d->t1 || !d->t2 || !d->a1 || !d->a2))
+        return fail(CMD_ERR_INVALID_ARG, "pulse arrays required when a drive direction is given");
+    if (drive && !(d->width != 0.0)) return fail(CMD_ERR_INVALID_ARG, "pulse width must be non-zero");
+    (void)h;
+    return CMD_OK;
+}
+
+int run_batch_device(cmd_handle* h, const cmd_batch_desc* d, const cmd::Pulse* d_pulses,
+                     cudaStream_t st, int32_t* launches) {
+    cmd::ResidentArgs a{};
+    a.G = (int)h->lay.G;
+    a.nonlocal = h->lay.Z - h->lay.LZ;
+    a.n_steps = d->n_steps;
+    a.save_every = d->save_interval;
+    a.T0 = d->T0;
+    a.dt = d->dt;
+    a.n_sites = (double)h->N;
+    a.nbr = h->nbr.as<int>();
+    a.y0 = d->states;
+    a.y0_stride = d->shared_initial ? 0 : h->N * 3;
+    a.y_out = d->final_states;
+    a.obs = d->obs;
+    a.rows = rows_for(d->n_steps, d->save_interval);
+    a.traj = nullptr;
+    a.pulses = d_pulses;
+    a.width = d->width;
+    a.freq = d->freq;
+    static const std::vector<double> zeros(3 * 64, 0.0);
+    const double* d1 = d->d1 ? d->d1 : zeros.data();
+    const double* d2 = d->d2 ? d->d2 : zeros.data();
+    if (int rc = launch_resident(h, a, nullptr, nullptr, d1, d2, d->B, st)) return rc;
+    if (launches) *launches = 1;
+    return CMD_OK;
+}
+
+}  // namespace
+
+int cmd_run_batch(cmd_handle* h, const cmd_batch_desc* d) {
+    cmd::clear_error();
+    if (int rc = check_handle(h, false)) return rc;
+    if (int rc = validate_batch(h, d)) return rc;
+    if (d->d1 || d->d2)
+        if (h->NA > 64) return fail(CMD_ERR_UNSUPPORTED, "drive directions limited to 64 atoms");
+    const int64_t B = d->B, N3 = h->N * 3;
+    const int64_t n_init = d->shared_initial ? 1 : B;
+    const int64_t rows = rows_for(d->n_steps, d->save_interval);
+    for (int64_t i = 0; i < n_init * N3; ++i)
+        if (!std::isfinite(d->states[i])) return fail(CMD_ERR_NONFINITE, "non-finite initial spin");
+    if (int rc = h->batch_states.ensure((size_t)(n_init + (d->final_states ? B : 0)) * N3 * sizeof(double))) return rc;
+    if (int rc = h->batch_out.ensure((size_t)B * rows * 10 * sizeof(double))) return rc;
+    double* d_init = h->batch_states.as<double>();
+    double* d_final = d->final_states ? d_init + n_init * N3 : nullptr;
+    CUDA_TRY(cudaMemcpyAsync(d_init, d->states, n_init * N3 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    const bool drive = d->d1 || d->d2;
+    cmd::Pulse* d_pulses = nullptr;
+    std::vector<cmd::Pulse> hp;
+    if (drive) {
+        hp.resize(B);
+        for (int64_t b = 0; b < B; ++b) hp[b] = cmd::Pulse{d->t1[b], d->t2[b], d->a1[b], d->a2[b]};
+        if (int rc = h->pulses.ensure(B * sizeof(cmd::Pulse))) return rc;
+        d_pulses = h->pulses.as<cmd::Pulse>();
+        CUDA_TRY(cudaMemcpyAsync(d_pulses, hp.data(), B * sizeof(cmd::Pulse), cudaMemcpyHostToDevice, h->stream));
+    }
+    cmd_batch_desc dd = *d;
+    dd.states = d_init;
+    dd.obs = h->batch_out.as<double>();
+    dd.final_states = d_final;
+    if (int rc = run_batch_device(h, &dd, d_pulses, h->stream, nullptr)) return rc;
+    CUDA_TRY(cudaMemcpyAsync(d->obs, dd.obs, B * rows * 10 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (d->final_states)
+        CUDA_TRY(cudaMemcpyAsync(d->final_states, d_final, B * N3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    return sync(h);
+}
+
+int cmd_run_batch_device(cmd_handle* h, const cmd_batch_desc* d, void* stream, int32_t* launches) {
+    cmd::clear_error();
+    if (launches) *launches = 0;
+    if (int rc = check_handle(h, false)) return rc;
+    if (int rc = validate_batch(h, d)) return rc;
+    cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+    if ((d->d1 || d->d2) && !d->pulse4)
+        return fail(CMD_ERR_INVALID_ARG, "driven device batch needs pulse4");
+    if ((d->d1 || d->d2) && h->NA > 64) return fail(CMD_ERR_UNSUPPORTED, "drive directions limited to 64 atoms");
+    const cmd::Pulse* d_pulses = (d->d1 || d->d2) ? reinterpret_cast<const cmd::Pulse*>(d->pulse4) : nullptr;
+    return run_batch_device(h, d, d_pulses, st, launches);
+}
+
+int cmd_plan_layout(const cmd_lattice_desc* d, int64_t* info) {
+    cmd::clear_error();
+    if (!d || !info) return fail(CMD_ERR_INVALID_ARG, "NULL argument");
+    for (int i = 0; i < 7; ++i) info[i] = 0;
+    if (d->spin_dim != 3 || d->lattice_size <= 0 || d->n_atoms <= 0 || !d->counts || !d->field || !d->onsite)
+        return fail(CMD_ERR_INVALID_ARG, "bad lattice description");
+    cmd_handle tmp;                    // host-side fields only; no stream, no device memory
+    tmp.N = d->lattice_size;
+    tmp.NA = d->n_atoms;
+    tmp.zmax = d->max_bilinear;
+    analyse(*d, tmp.lay);
+    info[0] = tmp.lay.NA;
+    info[1] = tmp.lay.G;
+    info[2] = tmp.lay.Z;
+    info[6] = tmp.lay.LZ;
+    const Layout& L = tmp.lay;
+    const int cpt = instance_cpt(pick_instance(L));
+    if (!cpt) return no_instance(L);
+    const int64_t threads = ((L.G + cpt - 1) / cpt + 31) / 32 * 32;
+    info[3] = threads;
+    info[4] = cpt;
+    info[5] = (int64_t)resident_smem(L.NA, L.G);
+    return CMD_OK;
+}
+
+int cmd_layout_info(cmd_handle* h, int64_t* info) {
+    cmd::clear_error();
+    if (int rc = check_handle(h, false)) return rc;
+    if (!info) return fail(CMD_ERR_INVALID_ARG, "NULL info");
+    for (int i = 0; i < 6; ++i) info[i] = 0;
+    info[0] = h->lay.NA;
+    info[1] = h->lay.G;
+    info[2] = h->lay.Z;
+    if (!h->lay.uniform) return fail(CMD_ERR_UNSUPPORTED, "lattice layout not supported: " + h->lay.why);
+    ResidentPlan plan;
+    cmd::ResidentArgs a{};
+    if (int rc = launch_resident(h, a, nullptr, nullptr, nullptr, nullptr, 0, h->stream, &plan)) return rc;
+    info[3] = plan.threads;
+    info[4] = plan.cpt;
+    info[5] = (int64_t)plan.smem;
+    return CMD_OK;
+}
+
+int cmd_integrate_batched(cmd_handle* h, const double* init, const double* tau2, int64_t B,
+                          const double* afm_signs, const double* frames, double T0, double T1,
+                          double dt, int64_t save_interval, int method, double* times, double* mags,
+                          int64_t max_rows, int64_t* rows_out) {
+    cmd::clear_error();
+    if (int rc = check_handle(h, false)) return rc;
+    if (!init || !tau2 || B <= 0) return fail(CMD_ERR_INVALID_ARG, "bad batch arguments");
+    if (method != CMD_RK4) return fail(CMD_ERR_UNSUPPORTED, "batched mode supports rk4 only (lattice_gpu.cu:781-784)");
+    if (save_interval <= 0 || !(dt > 0.0)) return fail(CMD_ERR_INVALID_ARG, "bad time grid");
+    std::vector<double> grid;
+    const int64_t n = count_steps(T0, T1, dt, 1e-12, &grid);
+    const int64_t rows = rows_for(n, save_interval);
+    if (rows_out) *rows_out = rows;
+    if (max_rows < rows) return fail(CMD_ERR_INVALID_ARG, "max_rows too small");
+    std::vector<double> t1(B, h->t1), a(B, h->amp), obs((size_t)B * rows * 10);
+    // Frames / AFM signs of the call override the lattice's for the observables.
+    std::vector<double> saved_frames = h->frames, saved_afm = h->afm;
+    if (frames) h->frames.assign(frames, frames + 9 * h->NA);
+    if (afm_signs) h->afm.assign(afm_signs, afm_signs + h->NA);
+    cmd_batch_desc d{};
+    d.B = B;
+    d.states = init;
+    d.shared_initial = 1;
+    d.method = CMD_RK4;
+    d.t1 = t1.data(); d.t2 = tau2; d.a1 = a.data(); d.a2 = a.data();
+    d.d1 = h->fd.data(); d.d2 = h->fd.data() + 3 * h->NA;
+    d.width = h->width; d.freq = h->freq;
+    d.T0 = T0; d.dt = dt;
+    d.n_steps = n; d.save_interval = save_interval;
+    d.obs = obs.data();
+    d.final_states = nullptr;
+    const int rc = cmd_run_batch(h, &d);
+    h->frames.swap(saved_frames);
+    h->afm.swap(saved_afm);
+    if (rc != CMD_OK) return rc;
+    if (times) {
+        int64_t r = 0;
+        for (int64_t k = 0; k < n; k += save_interval) times[r++] = grid[k];
+        times[r] = grid[n];
+    }
+    if (mags)
+        for (int64_t r = 0; r < rows; ++r)
+            for (int64_t b = 0; b < B; ++b)
+                std::memcpy(mags + (r * B + b) * 9, &obs[((size_t)b * rows + r) * 10], 9 * sizeof(double));
+    return CMD_OK;
+}
+
+}  // extern "C"

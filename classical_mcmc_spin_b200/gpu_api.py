@@ -1,0 +1,239 @@
+"""Python mirror of the reference's host GPU API for the LL MD path.
+
+Same function names, argument meaning and result layout as
+``namespace gpu`` in include/classical_spin/gpu/lattice_gpu_api.h
+(ze-bang/Classical_MCMC_Spin); the work happens in libcmd_b200.so on the GPU.
+Differences, by design: failures raise ``CmdError`` (the reference silently
+returns on a NULL handle or missing state, lattice_gpu.cu:660-723), the
+energy is implemented (the reference throws, lattice_gpu.cu:298-303), and an
+unknown method raises instead of falling back to ssprk53.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as nat
+from ._native import check, dptr, f64, iptr
+
+METHODS = {"rk4": nat.CMD_RK4, "dopri5": nat.CMD_DOPRI5_FIXED, "rk45": nat.CMD_RK45}
+
+
+def _method(method: str | int) -> int:
+    if isinstance(method, int):
+        return method
+    if method not in METHODS:
+        raise ValueError(f"unknown integration method {method!r}; supported: {sorted(METHODS)}")
+    return METHODS[method]
+
+
+class GPULatticeDataHandle:
+    """Opaque handle (lattice_gpu_api.h:30); owns a cmd_handle."""
+
+    def __init__(self, ptr: int, N: int, n_atoms: int):
+        self.ptr = C.c_void_p(ptr)
+        self.N = N
+        self.n_atoms = n_atoms
+
+    def close(self):
+        if self.ptr:
+            nat.lib().cmd_destroy(self.ptr)
+            self.ptr = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def layout_info(self) -> dict:
+        info = np.zeros(6, np.int64)
+        check(nat.lib().cmd_layout_info(self.ptr, iptr(info)), "cmd_layout_info")
+        return dict(sites_per_group=int(info[0]), groups=int(info[1]), bonds_per_site=int(info[2]),
+                    threads=int(info[3]), groups_per_thread=int(info[4]), smem_bytes=int(info[5]))
+
+
+def _desc(N, n_atoms, max_bilinear, field_, onsite, bilinear, partners, counts, frames=None, afm=None):
+    keep = dict(field=f64(field_, 3 * N), onsite=f64(onsite, 9 * N), bilinear=f64(bilinear, 9 * N * max_bilinear),
+                partners=np.ascontiguousarray(partners, dtype=np.int64),
+                counts=np.ascontiguousarray(counts, dtype=np.int64),
+                frames=None if frames is None else f64(frames, 9 * n_atoms),
+                afm=None if afm is None else f64(afm, n_atoms))
+    d = nat.LatticeDesc()
+    d.lattice_size = N
+    d.spin_dim = 3
+    d.n_atoms = n_atoms
+    d.max_bilinear = max_bilinear
+    d.field = dptr(keep["field"])
+    d.onsite = dptr(keep["onsite"])
+    d.bilinear = dptr(keep["bilinear"])
+    d.partners = iptr(keep["partners"])
+    d.counts = iptr(keep["counts"])
+    d.frames = dptr(keep["frames"]) if keep["frames"] is not None else None
+    d.afm_signs = dptr(keep["afm"]) if keep["afm"] is not None else None
+    return d, keep
+
+
+def create_gpu_lattice_data(lattice_size, spin_dim, N_atoms, max_bilinear, flat_field, flat_onsite,
+                            flat_bilinear, flat_partners, num_bilinear_per_site, sublattice_frames=None,
+                            afm_signs=None) -> GPULatticeDataHandle:
+    """create_gpu_lattice_data (lattice_gpu_api.h:47-57)."""
+    if spin_dim != 3:
+        raise ValueError("only spin_dim = 3 is supported")
+    d, _keep = _desc(int(lattice_size), int(N_atoms), int(max_bilinear), flat_field, flat_onsite, flat_bilinear,
+                     flat_partners, num_bilinear_per_site, sublattice_frames, afm_signs)
+    out = C.c_void_p()
+    check(nat.lib().cmd_create(C.byref(d), C.byref(out)), "create_gpu_lattice_data")
+    return GPULatticeDataHandle(out.value, int(lattice_size), int(N_atoms))
+
+
+def destroy_gpu_lattice_data(handle: GPULatticeDataHandle) -> None:
+    handle.close()
+
+
+def set_gpu_pulse(handle, flat_field_drive, pulse_amp, pulse_width, pulse_freq, t_pulse_1, t_pulse_2):
+    fd = f64(flat_field_drive, 6 * handle.n_atoms)
+    check(nat.lib().cmd_set_pulse(handle.ptr, dptr(fd), float(pulse_amp), float(pulse_width), float(pulse_freq),
+                                  float(t_pulse_1), float(t_pulse_2)), "set_gpu_pulse")
+
+
+def set_gpu_spins(handle, flat_spins):
+    s = f64(flat_spins, 3 * handle.N)
+    check(nat.lib().cmd_set_spins(handle.ptr, dptr(s), s.size), "set_gpu_spins")
+
+
+def get_gpu_spins(handle) -> np.ndarray:
+    s = np.zeros(3 * handle.N)
+    check(nat.lib().cmd_get_spins(handle.ptr, dptr(s), s.size), "get_gpu_spins")
+    return s
+
+
+def step_gpu(handle, t, dt, method="rk4"):
+    check(nat.lib().cmd_step(handle.ptr, float(t), float(dt), _method(method)), "step_gpu")
+
+
+def set_tolerances(handle, abs_tol, rel_tol, max_steps=0):
+    check(nat.lib().cmd_set_tolerances(handle.ptr, float(abs_tol), float(rel_tol), int(max_steps)),
+          "set_tolerances")
+
+
+def integrate_gpu(handle, T_start, T_end, dt, save_interval, method="rk4", with_states=True):
+    """integrate_gpu (lattice_gpu_api.h:117-125).
+
+    Returns ``(trajectory, obs)``: ``trajectory`` is the reference's list of
+    ``(t, state)`` pairs (empty when ``with_states`` is False) and ``obs`` the
+    per-row observables {M_af, M_local, M_global, E/N} computed on the device.
+    """
+    rows = C.c_int64()
+    m = _method(method)
+    rc = nat.lib().cmd_integrate(handle.ptr, float(T_start), float(T_end), float(dt), int(save_interval), m,
+                                 None, None, None, 0, C.byref(rows))
+    if rc not in (nat.CMD_OK, nat.CMD_ERR_INVALID_ARG) or rows.value <= 0:
+        check(rc, "integrate_gpu")
+    n = rows.value
+    times = np.zeros(n)
+    obs = np.zeros((n, 10))
+    states = np.zeros((n, 3 * handle.N)) if with_states else None
+    check(nat.lib().cmd_integrate(handle.ptr, float(T_start), float(T_end), float(dt), int(save_interval), m,
+                                  dptr(times), dptr(obs), dptr(states), n, C.byref(rows)), "integrate_gpu")
+    traj = [(float(times[r]), states[r]) for r in range(n)] if with_states else []
+    return traj, obs, times
+
+
+def compute_energy_gpu(handle) -> float:
+    e = C.c_double()
+    check(nat.lib().cmd_energy(handle.ptr, C.byref(e)), "compute_energy_gpu")
+    return e.value
+
+
+def normalize_spins_gpu(handle, spin_length):
+    check(nat.lib().cmd_normalize(handle.ptr, float(spin_length)), "normalize_spins_gpu")
+
+
+def compute_magnetization_gpu(handle):
+    ml = np.zeros(3)
+    ms = np.zeros(3)
+    check(nat.lib().cmd_magnetization(handle.ptr, dptr(ml), dptr(ms)), "compute_magnetization_gpu")
+    return ml, ms
+
+
+def observables_gpu(handle) -> np.ndarray:
+    row = np.zeros(10)
+    check(nat.lib().cmd_observables(handle.ptr, dptr(row)), "observables_gpu")
+    return row
+
+
+@dataclass
+class BatchedMagResult:
+    """BatchedMagResult (lattice_gpu_api.h:171-177)."""
+    B: int
+    spin_dim: int
+    n_time_points: int
+    times: np.ndarray = field(repr=False)
+    mag_data: np.ndarray = field(repr=False)   # [n_time_points][B][3][spin_dim]
+
+
+def integrate_gpu_batched(handle, flat_initial_state, tau2_values, afm_signs, sublattice_frames, T_start, T_end,
+                          dt, save_interval=1, method="rk4") -> BatchedMagResult:
+    """integrate_gpu_batched (lattice_gpu_api.h:205-214)."""
+    init = f64(flat_initial_state, 3 * handle.N)
+    tau2 = f64(tau2_values)
+    B = tau2.size
+    afm = None if afm_signs is None else f64(afm_signs, handle.n_atoms)
+    fr = None if sublattice_frames is None else f64(sublattice_frames, 9 * handle.n_atoms)
+    rows = C.c_int64()
+    m = _method(method)
+    rc = nat.lib().cmd_integrate_batched(handle.ptr, dptr(init), dptr(tau2), B, dptr(afm), dptr(fr),
+                                         float(T_start), float(T_end), float(dt), int(save_interval), m, None,
+                                         None, 0, C.byref(rows))
+    if rc not in (nat.CMD_OK, nat.CMD_ERR_INVALID_ARG) or rows.value <= 0:
+        check(rc, "integrate_gpu_batched")
+    n = rows.value
+    times = np.zeros(n)
+    mags = np.zeros((n, B, 3, 3))
+    check(nat.lib().cmd_integrate_batched(handle.ptr, dptr(init), dptr(tau2), B, dptr(afm), dptr(fr),
+                                          float(T_start), float(T_end), float(dt), int(save_interval), m,
+                                          dptr(times), dptr(mags), n, C.byref(rows)), "integrate_gpu_batched")
+    return BatchedMagResult(B=B, spin_dim=3, n_time_points=n, times=times, mag_data=mags)
+
+
+def run_batch(handle, states, n_steps, dt, T0=0.0, save_interval=1, t1=None, t2=None, a1=None, a2=None,
+              d1=None, d2=None, width=1.0, freq=0.0, shared_initial=False, want_final=True):
+    """Generalised batch (cmd_run_batch): per-trajectory pulse pairs, RK4.
+
+    Returns ``(obs[B][rows][10], final_states[B][N*3] or None)``.
+    """
+    st = f64(states)
+    B = st.size // (3 * handle.N) if not shared_initial else (len(t1) if t1 is not None else 1)
+    if shared_initial and st.size != 3 * handle.N:
+        raise ValueError("shared_initial needs one state of N*3 doubles")
+    if not shared_initial and st.size != B * 3 * handle.N:
+        raise ValueError("states must be [B][N*3]")
+    rows = int(nat.lib().cmd_batch_rows(int(n_steps), int(save_interval)))
+    obs = np.zeros((B, rows, 10))
+    fin = np.zeros((B, 3 * handle.N)) if want_final else None
+    keep = {}
+    d = nat.BatchDesc()
+    d.B = B
+    d.states = st.ctypes.data
+    d.shared_initial = int(bool(shared_initial))
+    d.method = nat.CMD_RK4
+    drive = d1 is not None or d2 is not None
+    if drive:
+        for name, arr, n in (("t1", t1, B), ("t2", t2, B), ("a1", a1, B), ("a2", a2, B),
+                             ("d1", d1 if d1 is not None else np.zeros(3 * handle.n_atoms), 3 * handle.n_atoms),
+                             ("d2", d2 if d2 is not None else np.zeros(3 * handle.n_atoms), 3 * handle.n_atoms)):
+            keep[name] = f64(arr, n)
+            setattr(d, name, keep[name].ctypes.data)
+    d.width = float(width)
+    d.freq = float(freq)
+    d.T0 = float(T0)
+    d.dt = float(dt)
+    d.n_steps = int(n_steps)
+    d.save_interval = int(save_interval)
+    d.obs = obs.ctypes.data
+    d.final_states = fin.ctypes.data if fin is not None else None
+    check(nat.lib().cmd_run_batch(handle.ptr, C.byref(d)), "cmd_run_batch")
+    return obs, fin

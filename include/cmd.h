@@ -1,0 +1,203 @@
+/*
+ * cmd.h -- C ABI of the B200 Landau-Lifshitz molecular-dynamics path.
+ *
+ * Drop-in replacement for the reference's host-side GPU boundary
+ * `namespace gpu` in include/classical_spin/gpu/lattice_gpu_api.h
+ * (ze-bang/Classical_MCMC_Spin).  That header passes std::vector / std::string
+ * and an opaque C++ handle; this one takes plain pointers and sizes, returns an
+ * int status from every call and never lets an exception cross the boundary.
+ *
+ * Conventions
+ *   - spin_dim is 3 (SU(2) spins); state arrays are the reference's flat
+ *     layout [site*3 + component], sites ordered ((i*d2+j)*d3+k)*n_atoms+atom.
+ *   - All numbers are FP64.
+ *   - A handle is not thread safe; different handles may be driven from
+ *     different host threads.  Each handle owns one CUDA stream.
+ *   - Observable rows are 10 doubles: {M_af[3], M_local[3], M_global[3], E/N}
+ *     with every magnetisation divided by N (the reference observers'
+ *     normalisation, src/core/lattice_md.cpp:406-422) and E/N the energy per
+ *     site of the static Hamiltonian (lattice.h:1485 total_energy_flat / N).
+ */
+#ifndef CMD_H
+#define CMD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (the reference throws std::runtime_error or silently no-ops,
+ * lattice_gpu.cu:660-723 and gpu_common_helpers.cuh:15-32). */
+enum {
+    CMD_OK = 0,
+    CMD_ERR_INVALID_ARG = 1,
+    CMD_ERR_UNSUPPORTED = 2,
+    CMD_ERR_CUDA = 3,
+    CMD_ERR_NONFINITE = 4,
+    CMD_ERR_WATCHDOG = 5,
+    CMD_ERR_OOM = 6,
+    CMD_ERR_STATE = 7
+};
+
+/* Integration methods.  The reference GPU API takes a method string
+ * (lattice_gpu_api.h:101-125); "rk4" and "dopri5" are the ones on this path.
+ *   CMD_RK4          classic fixed-step RK4 (integrator.cuh:115-139)
+ *   CMD_DOPRI5_FIXED Dormand-Prince 5 tableau, fixed step, no error control
+ *                    (the reference GPU "dopri5", integrator.cuh:186-228)
+ *   CMD_RK45         controlled Dormand-Prince 5(4) with the CPU path's
+ *                    Boost.Odeint step control (lattice.h:4072-4078)      */
+enum { CMD_RK4 = 0, CMD_DOPRI5_FIXED = 1, CMD_RK45 = 2 };
+
+typedef struct cmd_handle cmd_handle;
+
+/*
+ * Lattice in the reference's flattened GPU-boundary form
+ * (create_gpu_lattice_data, lattice_gpu_api.h:47-57; filled by
+ * Lattice::ensure_gpu_data_initialized, lattice.h:5429-5497), plus the
+ * sublattice frames and AFM signs that the reference passes separately to
+ * integrate_gpu_batched (lattice_gpu_api.h:205-214).
+ */
+typedef struct cmd_lattice_desc {
+    int64_t lattice_size;        /* N                                          */
+    int32_t spin_dim;            /* must be 3                                  */
+    int32_t n_atoms;             /* atoms per unit cell                        */
+    int32_t max_bilinear;        /* ELL width                                  */
+    int32_t reserved;
+    const double* field;         /* [N*3]                                      */
+    const double* onsite;        /* [N*9]                                      */
+    const double* bilinear;      /* [N*max_bilinear*9] row-major J per entry   */
+    const int64_t* partners;     /* [N*max_bilinear]                           */
+    const int64_t* counts;       /* [N] valid entries per site                 */
+    const double* frames;        /* [n_atoms*9] or NULL (identity)             */
+    const double* afm_signs;     /* [n_atoms]   or NULL (all +1)               */
+} cmd_lattice_desc;
+
+/* create_gpu_lattice_data (lattice_gpu_api.h:47-57). */
+int cmd_create(const cmd_lattice_desc* desc, cmd_handle** out);
+/* destroy_gpu_lattice_data (lattice_gpu_api.h:62). */
+int cmd_destroy(cmd_handle* h);
+
+/* set_gpu_pulse (lattice_gpu_api.h:67-75): field_drive [2*n_atoms*3], already
+ * rotated by the sublattice frames (Lattice::set_pulse, lattice_md.cpp:210-224). */
+int cmd_set_pulse(cmd_handle* h, const double* field_drive, double amp, double width,
+                  double freq, double t_pulse_1, double t_pulse_2);
+
+/* set_gpu_spins / get_gpu_spins (lattice_gpu_api.h:83-97); n = N*3. */
+int cmd_set_spins(cmd_handle* h, const double* spins, int64_t n);
+int cmd_get_spins(cmd_handle* h, double* spins, int64_t n);
+
+/* step_gpu (lattice_gpu_api.h:135-140): one step of `method` from time t. */
+int cmd_step(cmd_handle* h, double t, double dt, int method);
+
+/*
+ * integrate_gpu (lattice_gpu_api.h:117-125).  Fixed-step methods follow the
+ * reference loop: t = T0; while (t < T1) { if (k % save_interval == 0) save;
+ * step; t += dt; ++k; } save.  CMD_RK45 follows the CPU controller and saves
+ * every accepted step (dt is the initial step, tolerances from
+ * cmd_set_tolerances).  Per saved row: times[r], obs[r*10..], and, when
+ * `states` is non-NULL, the full state states[r*N*3..] (the reference's
+ * trajectory vector).  *rows_out gets the number of rows; CMD_ERR_INVALID_ARG
+ * if max_rows is too small (rows_out still gets the count needed).
+ */
+int cmd_integrate(cmd_handle* h, double T0, double T1, double dt, int64_t save_interval,
+                  int method, double* times, double* obs, double* states, int64_t max_rows,
+                  int64_t* rows_out);
+
+/* Controlled-stepper tolerances (SpinConfig md_abs_tol / md_rel_tol) and the
+ * accepted-step cap for CMD_RK45. */
+int cmd_set_tolerances(cmd_handle* h, double abs_tol, double rel_tol, int64_t max_steps);
+
+/* compute_energy_gpu (lattice_gpu_api.h:145; unimplemented in the reference):
+ * total energy of the current state, same terms as total_energy_flat. */
+int cmd_energy(cmd_handle* h, double* energy);
+
+/* normalize_spins_gpu (lattice_gpu_api.h:150). */
+int cmd_normalize(cmd_handle* h, double spin_length);
+
+/* compute_magnetization_gpu (lattice_gpu_api.h:155-159): mean spin and the
+ * (-1)^i staggered mean (lattice_gpu.cu:729-760), each [3]. */
+int cmd_magnetization(cmd_handle* h, double* mag_local, double* mag_staggered);
+
+/* Observables of the current state: one 10-double row (see top of file). */
+int cmd_observables(cmd_handle* h, double* row);
+
+/*
+ * integrate_gpu_batched (lattice_gpu_api.h:171-214): B replicas of this
+ * lattice from one initial state, replica b with second-pulse time tau2[b]
+ * and every other pulse parameter from cmd_set_pulse.  Loop:
+ * while (t < T1 - 1e-12), saving every save_interval steps and at the end.
+ * mags[r][b][m][d] (m = 0 M_af, 1 M_local, 2 M_global), each / N.
+ * afm_signs / frames may be NULL to use the lattice's own.
+ */
+int cmd_integrate_batched(cmd_handle* h, const double* initial_state, const double* tau2,
+                          int64_t B, const double* afm_signs, const double* frames,
+                          double T0, double T1, double dt, int64_t save_interval,
+                          int method, double* times, double* mags, int64_t max_rows,
+                          int64_t* rows_out);
+
+/*
+ * Generalised batch (no reference counterpart; it is the batched 2DCS scan
+ * with pump-only / probe-only / pump+probe trajectories in one launch).
+ * Trajectory b starts from states[b] (or from states[0] for every b when
+ * shared_initial != 0), with drive
+ *   H -= a1[b] env(t - t1[b]) d1 + a2[b] env(t - t2[b]) d2,
+ *   env(x) = exp(-(x / (2 width))^2) cos(freq x)
+ * where d1/d2 are the frame-rotated pulse directions [n_atoms*3] (NULL: no
+ * drive).  RK4, `n_steps` steps of dt from T0 (t += dt), one row of obs every
+ * `save_interval` steps plus the final state: obs[b][row][10].  Final states
+ * are written back into `final_states` when non-NULL.  Host pointers.
+ */
+typedef struct cmd_batch_desc {
+    int64_t B;
+    const double* states;        /* [B or 1][N*3]                              */
+    int32_t shared_initial;
+    int32_t method;              /* CMD_RK4                                    */
+    const double* t1; const double* t2;   /* [B]                               */
+    const double* a1; const double* a2;   /* [B] pulse amplitudes              */
+    const double* d1; const double* d2;   /* [n_atoms*3] or NULL               */
+    double width, freq;
+    double T0, dt;
+    int64_t n_steps, save_interval;
+    double* obs;                 /* [B][rows][10]; rows = n_steps/save + 1 (+1 if n_steps%save) */
+    double* final_states;        /* [B][N*3] or NULL                           */
+    const double* pulse4;        /* cmd_run_batch_device only: device [B][4] =
+                                    {t1, t2, a1, a2} (t1..a2 above are unused) */
+} cmd_batch_desc;
+int cmd_run_batch(cmd_handle* h, const cmd_batch_desc* d);
+/* Rows cmd_run_batch writes per trajectory. */
+int64_t cmd_batch_rows(int64_t n_steps, int64_t save_interval);
+
+/*
+ * Device-resident variant of cmd_run_batch for callers that keep their data
+ * on the GPU (the torch layer, the benchmark): states, obs, final_states and
+ * pulse4 are device pointers; d1/d2 stay host arrays (they become kernel
+ * parameters).  The call is asynchronous on `stream` (a cudaStream_t, NULL =
+ * the handle's stream).  `launches` (may be NULL) gets the number of kernels
+ * launched.
+ */
+int cmd_run_batch_device(cmd_handle* h, const cmd_batch_desc* d, void* stream, int32_t* launches);
+
+/* Lattice layout chosen at cmd_create (for diagnostics and the autotuner):
+ * info[0] = sites per group (unit-cell atoms), info[1] = groups,
+ * info[2] = max bonds per site kept, info[3] = threads per block of the
+ * resident RK4 kernel, info[4] = groups per thread, info[5] = shared-memory
+ * bytes per trajectory. */
+int cmd_layout_info(cmd_handle* h, int64_t* info);
+
+/* Host-only version of the layout analysis cmd_create performs (no CUDA
+ * call): fills info[0..5] like cmd_layout_info, info[6] = leading local slots
+ * per atom; returns CMD_ERR_UNSUPPORTED with the reason when no resident
+ * kernel covers the lattice. */
+int cmd_plan_layout(const cmd_lattice_desc* desc, int64_t* info);
+
+/* Message for the last non-OK status on this host thread. */
+const char* cmd_last_error(void);
+/* Library version string. */
+const char* cmd_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
