@@ -231,6 +231,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
+    ap.add_argument("--no-peak", action="store_true", help="skip the DGEMM peak probe (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -283,9 +284,14 @@ def main():
     desc.final_states = d_fin.data_ptr()
     desc.pulse4 = d_pulse.data_ptr()
     launches = C.c_int32()
+    # A dedicated stream: the kernel, the L2 flush and every CUDA event below go
+    # to this one stream, so the events bracket exactly the launched work.
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
 
     def launch():
         st = torch.cuda.current_stream(dev).cuda_stream
+        assert st != 0
         nat.check(nat.lib().cmd_run_batch_device(h.ptr, C.byref(desc), C.c_void_p(st), C.byref(launches)),
                   "cmd_run_batch_device")
 
@@ -387,7 +393,7 @@ def main():
                              "M and E every step, via integrate_gpu (host buffers)"}
 
     peaks = measured_peaks()
-    fp64 = fp64_peak_tflops(torch) if rank == 0 else None
+    fp64 = fp64_peak_tflops(torch) if (rank == 0 and not args.no_peak) else None
     achieved_tflops = FLOPS_PER_SPIN_STEP * B * N * S / (kernel_ms * 1e-3) / 1e12
     traffic = profile_traffic()
     roofline = {"bound": "fp64", "achieved": achieved_tflops, "peak": fp64, "unit": "TFLOP/s",

@@ -91,12 +91,14 @@ struct cmd_handle {
     int64_t N = 0;
     int NA = 0;
     int zmax = 0;
-    std::vector<double> field, onsite, frames, afm;   // field/onsite per site; frames/afm per atom
+    std::vector<double> field, onsite, frames, afm;   // per atom
     bool has_field = false, has_onsite = false;
     Layout lay;
     cudaStream_t stream = nullptr;
     DevBuf state, nbr, obs, traj, batch_states, batch_out, pulses, scratch;
+    DevBuf dframes, dafm, times, drive, raw, tune_states, tune_obs;
     bool has_state = false;
+    int variant = -1;           // resident-kernel variant; -1 = heuristic default
     // pulse (set_gpu_pulse)
     std::vector<double> fd;     // [2][NA*3]
     double amp = 0.0, width = 1.0, freq = 0.0, t1 = 0.0, t2 = 0.0;
@@ -232,9 +234,10 @@ void analyse(const cmd_lattice_desc& d, Layout& L) {
     L.why = "coupling table is not identical in every unit cell";
 }
 
+int64_t rows_for(int64_t n_steps, int64_t save) { return (n_steps + save - 1) / save + 1; }
+
 template <int NAT, int Z>
-void fill_couplings(const cmd_handle* h, const double* frames, const double* afm, const double* d1,
-                    const double* d2, cmd::Couplings<NAT, Z>& cp) {
+void fill_couplings(const cmd_handle* h, const double* d1, const double* d2, cmd::Couplings<NAT, Z>& cp) {
     std::memset(&cp, 0, sizeof(cp));
     const Layout& L = h->lay;
     for (int a = 0; a < NAT; ++a) {
@@ -243,8 +246,6 @@ void fill_couplings(const cmd_handle* h, const double* frames, const double* afm
         cp.zc[a] = L.zc[a];
         std::memcpy(cp.field[a], &h->field[3 * a], 3 * sizeof(double));
         std::memcpy(cp.onsite[a], &h->onsite[9 * a], 9 * sizeof(double));
-        std::memcpy(cp.frame[a], (frames ? frames : h->frames.data()) + 9 * a, 9 * sizeof(double));
-        cp.afm[a] = (afm ? afm : h->afm.data())[a];
         if (d1) std::memcpy(cp.d1[a], d1 + 3 * a, 3 * sizeof(double));
         if (d2) std::memcpy(cp.d2[a], d2 + 3 * a, 3 * sizeof(double));
     }
@@ -252,24 +253,21 @@ void fill_couplings(const cmd_handle* h, const double* frames, const double* afm
     cp.has_onsite = h->has_onsite;
 }
 
-struct ResidentPlan {
-    int threads = 0, cpt = 0;
-    size_t smem = 0;
-};
-
 size_t resident_smem(int NA, int64_t G) {
-    return (size_t)2 * NA * 3 * G * sizeof(double) + (32 * cmd::kRedStride + 16 + 12) * sizeof(double);
+    return (size_t)2 * NA * 3 * G * sizeof(double) + (32 * cmd::kRedStride + 12) * sizeof(double);
 }
 
-template <int NAT, int Z, int LZ, int CPT, int MAXT>
-int launch_one(const cmd_handle* h, const cmd::ResidentArgs& args, const double* frames,
-               const double* afm, const double* d1, const double* d2, int64_t B,
-               cudaStream_t st, ResidentPlan* plan) {
-    auto kern = cmd::rk4_resident_kernel<NAT, Z, LZ, CPT, MAXT>;
+using LaunchFn = int (*)(const cmd_handle*, const cmd::ResidentArgs&, const double*, const double*, int64_t,
+                         cudaStream_t);
+
+template <int NAT, int Z, int LZ, int CPT, int MAXT, int MINB, bool YREG>
+int launch_one(const cmd_handle* h, const cmd::ResidentArgs& args, const double* d1, const double* d2,
+               int64_t B, cudaStream_t st) {
+    auto kern = cmd::rk4_resident_kernel<NAT, Z, LZ, CPT, MAXT, MINB, YREG>;
     const int64_t G = h->lay.G;
     int threads = (int)((G + CPT - 1) / CPT);
     threads = ((threads + 31) / 32) * 32;
-    if (threads > MAXT) return fail(CMD_ERR_UNSUPPORTED, "lattice too large for the resident kernel");
+    if (threads > MAXT) return fail(CMD_ERR_UNSUPPORTED, "lattice too large for this kernel variant");
     const size_t smem = resident_smem(NAT, G);
     if (smem > kMaxSmem) return fail(CMD_ERR_UNSUPPORTED, "stage buffers exceed shared memory");
     static bool attr_set = false;
@@ -277,31 +275,60 @@ int launch_one(const cmd_handle* h, const cmd::ResidentArgs& args, const double*
         CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
         attr_set = true;
     }
-    if (plan) { plan->threads = threads; plan->cpt = CPT; plan->smem = smem; }
-    if (B <= 0) return CMD_OK;      // plan only
     cmd::Couplings<NAT, Z> cp;
-    fill_couplings<NAT, Z>(h, frames, afm, d1, d2, cp);
+    fill_couplings<NAT, Z>(h, d1, d2, cp);
     kern<<<(unsigned)B, threads, smem, st>>>(cp, args);
     CUDA_TRY(cudaGetLastError());
     return CMD_OK;
 }
 
-// Resident-kernel instances compiled into the library.
-enum Instance { kNone = 0, kHoney1, kHoney2, kPyro1, kPyro2 };
+// Resident-kernel variants compiled into the library: (atoms/cell, bonds/atom,
+// in-cell bonds) x (cells per thread, max threads, min CTAs per SM, own stage
+// input kept in registers).  The autotuner times the ones that fit a lattice.
+struct Variant {
+    int NAT, Z, LZ, CPT, MAXT, MINB;
+    bool YREG;
+    LaunchFn fn;
+    const char* name;
+};
 
-Instance pick_instance(const Layout& L) {
-    if (!L.uniform) return kNone;
-    if (L.NA == 2 && L.Z == 3 && L.LZ == 1) {
-        if (L.G <= 640) return kHoney1;
-        if (L.G <= 1024) return kHoney2;
-    } else if (L.NA == 4 && L.Z == 6 && L.LZ == 3) {
-        if (L.G <= 512) return kPyro1;
-        if (L.G <= 1024) return kPyro2;
-    }
-    return kNone;
+#define CMD_VARIANT(NAT, Z, LZ, CPT, MAXT, MINB, YREG) \
+    Variant{NAT, Z, LZ, CPT, MAXT, MINB, YREG, &launch_one<NAT, Z, LZ, CPT, MAXT, MINB, YREG>, \
+            "rk4_resident<" #NAT "," #Z "," #LZ "> cpt=" #CPT " maxt=" #MAXT " minb=" #MINB " yreg=" #YREG}
+
+const Variant kVariants[] = {
+    // 2-atom cells with 3 bonds per site (Kitaev / Heisenberg honeycomb)
+    CMD_VARIANT(2, 3, 1, 1, 640, 1, true),
+    CMD_VARIANT(2, 3, 1, 2, 320, 2, false),
+    CMD_VARIANT(2, 3, 1, 3, 192, 3, false),
+    CMD_VARIANT(2, 3, 1, 4, 160, 3, false),
+    CMD_VARIANT(2, 3, 1, 4, 160, 3, true),
+    CMD_VARIANT(2, 3, 1, 6, 96, 3, true),
+    CMD_VARIANT(2, 3, 1, 2, 512, 1, true),
+    CMD_VARIANT(2, 3, 1, 4, 256, 2, false),
+    // 4-atom cells with 6 bonds per site (nearest-neighbour pyrochlore)
+    CMD_VARIANT(4, 6, 3, 1, 512, 1, true),
+    CMD_VARIANT(4, 6, 3, 2, 256, 2, false),
+    CMD_VARIANT(4, 6, 3, 2, 512, 1, false),
+};
+constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
+
+bool variant_fits(const Variant& v, const Layout& L) {
+    if (!L.uniform || v.NAT != L.NA || v.Z != L.Z || v.LZ != L.LZ) return false;
+    const int64_t threads = ((L.G + v.CPT - 1) / v.CPT + 31) / 32 * 32;
+    if (threads > v.MAXT) return false;
+    const size_t smem = resident_smem(v.NAT, L.G);
+    if (smem > kMaxSmem) return false;
+    return true;
 }
 
-int instance_cpt(Instance i) { return (i == kHoney2 || i == kPyro2) ? 2 : (i == kNone ? 0 : 1); }
+// Variant used when the caller did not pick one: the first fitting entry of
+// the table (entries are ordered by preference for a lone trajectory).
+int default_variant(const Layout& L) {
+    for (int i = 0; i < kNumVariants; ++i)
+        if (variant_fits(kVariants[i], L)) return i;
+    return -1;
+}
 
 int no_instance(const Layout& L) {
     if (!L.uniform) return fail(CMD_ERR_UNSUPPORTED, "lattice layout not supported: " + L.why);
@@ -312,20 +339,108 @@ int no_instance(const Layout& L) {
     return fail(CMD_ERR_UNSUPPORTED, buf);
 }
 
-// Launches the kernel instance for the handle's layout; B = 0 only fills `plan`.
-int launch_resident(const cmd_handle* h, const cmd::ResidentArgs& args, const double* frames,
-                    const double* afm, const double* d1, const double* d2, int64_t B,
-                    cudaStream_t st, ResidentPlan* plan = nullptr) {
-    switch (pick_instance(h->lay)) {
-        case kHoney1: return launch_one<2, 3, 1, 1, 640>(h, args, frames, afm, d1, d2, B, st, plan);
-        case kHoney2: return launch_one<2, 3, 1, 2, 512>(h, args, frames, afm, d1, d2, B, st, plan);
-        case kPyro1: return launch_one<4, 6, 3, 1, 512>(h, args, frames, afm, d1, d2, B, st, plan);
-        case kPyro2: return launch_one<4, 6, 3, 2, 512>(h, args, frames, afm, d1, d2, B, st, plan);
-        default: return no_instance(h->lay);
-    }
+int pick_variant(const cmd_handle* h) {
+    if (h->variant >= 0 && h->variant < kNumVariants && variant_fits(kVariants[h->variant], h->lay))
+        return h->variant;
+    return default_variant(h->lay);
 }
 
-int64_t rows_for(int64_t n_steps, int64_t save) { return (n_steps + save - 1) / save + 1; }
+// Everything one resident run needs besides the handle.
+struct RunSpec {
+    int64_t B = 1;
+    const double* y0 = nullptr;       // device
+    int64_t y0_stride = 0;
+    double* y_out = nullptr;          // device
+    double* obs = nullptr;            // device [B][rows][10]
+    double* traj = nullptr;           // device [B][rows][N*3]
+    double T0 = 0.0, dt = 0.0;
+    int64_t n_steps = 0, save = 1;
+    const cmd::Pulse* pulses = nullptr;   // device [B]
+    double width = 1.0, freq = 0.0;
+    const double* d1 = nullptr;       // host [NA*3]
+    const double* d2 = nullptr;
+    const double* frames = nullptr;   // device [NA*9]
+    const double* afm = nullptr;      // device [NA]
+    double n_sites = 1.0;
+    int variant = -1;                 // -1: handle's choice
+};
+
+template <int NAT>
+void launch_finish(const double* raw, int64_t stride, int64_t n, const double* fr, const double* afm,
+                   double n_sites, double* obs, cudaStream_t st) {
+    const int blocks = (int)std::min<int64_t>((n + 255) / 256, 4096);
+    cmd::finish_rows_kernel<NAT><<<std::max(blocks, 1), 256, 0, st>>>(raw, stride, n, fr, afm, n_sites, obs);
+}
+
+// Launches drive-table pre-pass (when driven), the resident kernel and the
+// row-finishing post-pass on `st`.  Asynchronous; returns the launch count.
+int run_resident(cmd_handle* h, const RunSpec& r, cudaStream_t st, int32_t* launches) {
+    int32_t nl = 0;
+    const int vi = r.variant >= 0 ? r.variant : pick_variant(h);
+    if (vi < 0 || !variant_fits(kVariants[vi], h->lay)) return no_instance(h->lay);
+    const Variant& V = kVariants[vi];
+    const int64_t rows = rows_for(r.n_steps, r.save);
+    const int NR = 3 * V.NAT + 1;
+    cmd::ResidentArgs a{};
+    a.G = (int)h->lay.G;
+    a.n_steps = r.n_steps;
+    a.save_every = r.save;
+    a.T0 = r.T0;
+    a.dt = r.dt;
+    a.nbr = h->nbr.as<int>();
+    a.y0 = r.y0;
+    a.y0_stride = r.y0_stride;
+    a.y_out = r.y_out;
+    a.rows = rows;
+    a.traj = r.traj;
+    a.drive = nullptr;
+    if (r.obs) {
+        if (NR <= 10) {
+            a.raw = r.obs;
+            a.raw_stride = 10;
+        } else {
+            if (int rc = h->raw.ensure((size_t)r.B * rows * NR * sizeof(double))) return rc;
+            a.raw = h->raw.as<double>();
+            a.raw_stride = NR;
+        }
+    }
+    if (r.pulses && r.n_steps > 0) {
+        std::vector<double> grid;
+        grid.reserve(r.n_steps + 1);
+        double t = r.T0;
+        for (int64_t k = 0; k < r.n_steps; ++k) {     // t_k of the reference loop (t += dt)
+            grid.push_back(t);
+            t += r.dt;
+        }
+        if (int rc = h->times.ensure(grid.size() * sizeof(double))) return rc;
+        if (int rc = h->drive.ensure((size_t)r.B * r.n_steps * 6 * sizeof(double))) return rc;
+        CUDA_TRY(cudaMemcpyAsync(h->times.p, grid.data(), grid.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+        const int64_t total = r.B * r.n_steps * 6;
+        const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 32);
+        cmd::drive_table_kernel<<<blocks, 256, 0, st>>>(r.pulses, h->times.as<double>(), r.n_steps, r.dt, r.width,
+                                                       r.freq, r.B, h->drive.as<double>());
+        CUDA_TRY(cudaGetLastError());
+        ++nl;
+        a.drive = h->drive.as<double>();
+    }
+    static const std::vector<double> zeros(3 * 64, 0.0);
+    if (int rc = V.fn(h, a, r.d1 ? r.d1 : zeros.data(), r.d2 ? r.d2 : zeros.data(), r.B, st)) return rc;
+    ++nl;
+    if (r.obs) {
+        const int64_t n = r.B * rows;
+        const double* fr = r.frames ? r.frames : h->dframes.as<double>();
+        const double* af = r.afm ? r.afm : h->dafm.as<double>();
+        switch (V.NAT) {
+            case 2: launch_finish<2>(a.raw, a.raw_stride, n, fr, af, r.n_sites, r.obs, st); break;
+            case 4: launch_finish<4>(a.raw, a.raw_stride, n, fr, af, r.n_sites, r.obs, st); break;
+            default: return fail(CMD_ERR_UNSUPPORTED, "no row finisher for this cell size");
+        }
+        CUDA_TRY(cudaGetLastError());
+        ++nl;
+    }
+    if (launches) *launches = nl;
+    return CMD_OK;
+}
 
 // Reference GPU loop (integrator.cuh:477-483): number of steps and times.
 int64_t count_steps(double T0, double T1, double dt, double margin, std::vector<double>* times) {
@@ -380,6 +495,14 @@ __global__ void magnetization_kernel(const double* s, int64_t N, double* out) {
     }
     if (threadIdx.x == 0)
         for (int q = 0; q < 6; ++q) out[q] = sh[q][0] / (double)N;
+}
+
+int upload_frames(cmd_handle* h, const double* frames, const double* afm) {
+    if (int rc = h->dframes.ensure(9 * (size_t)h->NA * sizeof(double))) return rc;
+    if (int rc = h->dafm.ensure((size_t)h->NA * sizeof(double))) return rc;
+    CUDA_TRY(cudaMemcpyAsync(h->dframes.p, frames, 9 * h->NA * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(h->dafm.p, afm, h->NA * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    return sync(h);
 }
 
 int check_handle(cmd_handle* h, bool need_state) {
@@ -441,6 +564,7 @@ int cmd_create(const cmd_lattice_desc* d, cmd_handle** out) {
             rc = fail(CMD_ERR_CUDA, "neighbour table upload failed");
     }
     if (rc == CMD_OK) rc = h->state.ensure((size_t)h->N * 3 * sizeof(double));
+    if (rc == CMD_OK) rc = upload_frames(h, h->frames.data(), h->afm.data());
     if (rc != CMD_OK) {
         cmd_destroy(h);
         return rc;
@@ -453,7 +577,8 @@ int cmd_destroy(cmd_handle* h) {
     if (!h) return CMD_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (DevBuf* b : {&h->state, &h->nbr, &h->obs, &h->traj, &h->batch_states, &h->batch_out,
-                      &h->pulses, &h->scratch})
+                      &h->pulses, &h->scratch, &h->dframes, &h->dafm, &h->times, &h->drive, &h->raw,
+                      &h->tune_states, &h->tune_obs})
         b->release();
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -511,32 +636,29 @@ int run_single(cmd_handle* h, double T0, double dt, int64_t n_steps, int64_t sav
         if (int rc = h->obs.ensure((size_t)rows * 10 * sizeof(double))) return rc;
     if (want_traj)
         if (int rc = h->traj.ensure((size_t)rows * h->N * 3 * sizeof(double))) return rc;
+    const bool driven = with_pulse && h->amp != 0.0;
     cmd::Pulse pl{h->t1, h->t2, h->amp, h->amp};
-    if (with_pulse && h->amp != 0.0) {
+    if (driven) {
         if (int rc = h->pulses.ensure(sizeof(cmd::Pulse))) return rc;
         CUDA_TRY(cudaMemcpyAsync(h->pulses.p, &pl, sizeof(pl), cudaMemcpyHostToDevice, h->stream));
     }
-    cmd::ResidentArgs a{};
-    a.G = (int)h->lay.G;
-    a.nonlocal = h->lay.Z - h->lay.LZ;
-    a.n_steps = n_steps;
-    a.save_every = save;
-    a.T0 = T0;
-    a.dt = dt;
-    a.n_sites = n_sites;
-    a.nbr = h->nbr.as<int>();
-    a.y0 = h->state.as<double>();
-    a.y0_stride = 0;
-    a.y_out = h->state.as<double>();
-    a.obs = want_obs ? h->obs.as<double>() : nullptr;
-    a.rows = rows;
-    a.traj = want_traj ? h->traj.as<double>() : nullptr;
-    a.pulses = (with_pulse && h->amp != 0.0) ? h->pulses.as<cmd::Pulse>() : nullptr;
-    a.width = h->width;
-    a.freq = h->freq;
-    const double* d1 = h->fd.data();
-    const double* d2 = h->fd.data() + 3 * h->NA;
-    if (int rc = launch_resident(h, a, nullptr, nullptr, d1, d2, 1, h->stream)) return rc;
+    RunSpec r;
+    r.B = 1;
+    r.y0 = h->state.as<double>();
+    r.y_out = h->state.as<double>();
+    r.obs = want_obs ? h->obs.as<double>() : nullptr;
+    r.traj = want_traj ? h->traj.as<double>() : nullptr;
+    r.T0 = T0;
+    r.dt = dt;
+    r.n_steps = n_steps;
+    r.save = save;
+    r.pulses = driven ? h->pulses.as<cmd::Pulse>() : nullptr;
+    r.width = h->width;
+    r.freq = h->freq;
+    r.d1 = h->fd.data();
+    r.d2 = h->fd.data() + 3 * h->NA;
+    r.n_sites = n_sites;
+    if (int rc = run_resident(h, r, h->stream, nullptr)) return rc;
     return sync(h);
 }
 
@@ -644,30 +766,23 @@ int validate_batch(const cmd_handle* h, const cmd_batch_desc* d) {
 
 int run_batch_device(cmd_handle* h, const cmd_batch_desc* d, const cmd::Pulse* d_pulses,
                      cudaStream_t st, int32_t* launches) {
-    cmd::ResidentArgs a{};
-    a.G = (int)h->lay.G;
-    a.nonlocal = h->lay.Z - h->lay.LZ;
-    a.n_steps = d->n_steps;
-    a.save_every = d->save_interval;
-    a.T0 = d->T0;
-    a.dt = d->dt;
-    a.n_sites = (double)h->N;
-    a.nbr = h->nbr.as<int>();
-    a.y0 = d->states;
-    a.y0_stride = d->shared_initial ? 0 : h->N * 3;
-    a.y_out = d->final_states;
-    a.obs = d->obs;
-    a.rows = rows_for(d->n_steps, d->save_interval);
-    a.traj = nullptr;
-    a.pulses = d_pulses;
-    a.width = d->width;
-    a.freq = d->freq;
-    static const std::vector<double> zeros(3 * 64, 0.0);
-    const double* d1 = d->d1 ? d->d1 : zeros.data();
-    const double* d2 = d->d2 ? d->d2 : zeros.data();
-    if (int rc = launch_resident(h, a, nullptr, nullptr, d1, d2, d->B, st)) return rc;
-    if (launches) *launches = 1;
-    return CMD_OK;
+    RunSpec r;
+    r.B = d->B;
+    r.y0 = d->states;
+    r.y0_stride = d->shared_initial ? 0 : h->N * 3;
+    r.y_out = d->final_states;
+    r.obs = d->obs;
+    r.T0 = d->T0;
+    r.dt = d->dt;
+    r.n_steps = d->n_steps;
+    r.save = d->save_interval;
+    r.pulses = d_pulses;
+    r.width = d->width;
+    r.freq = d->freq;
+    r.d1 = d->d1;
+    r.d2 = d->d2;
+    r.n_sites = (double)h->N;
+    return run_resident(h, r, st, launches);
 }
 
 }  // namespace
@@ -738,11 +853,11 @@ int cmd_plan_layout(const cmd_lattice_desc* d, int64_t* info) {
     info[2] = tmp.lay.Z;
     info[6] = tmp.lay.LZ;
     const Layout& L = tmp.lay;
-    const int cpt = instance_cpt(pick_instance(L));
-    if (!cpt) return no_instance(L);
-    const int64_t threads = ((L.G + cpt - 1) / cpt + 31) / 32 * 32;
-    info[3] = threads;
-    info[4] = cpt;
+    const int vi = default_variant(L);
+    if (vi < 0) return no_instance(L);
+    const Variant& V = kVariants[vi];
+    info[3] = ((L.G + V.CPT - 1) / V.CPT + 31) / 32 * 32;
+    info[4] = V.CPT;
     info[5] = (int64_t)resident_smem(L.NA, L.G);
     return CMD_OK;
 }
@@ -755,13 +870,92 @@ int cmd_layout_info(cmd_handle* h, int64_t* info) {
     info[0] = h->lay.NA;
     info[1] = h->lay.G;
     info[2] = h->lay.Z;
-    if (!h->lay.uniform) return fail(CMD_ERR_UNSUPPORTED, "lattice layout not supported: " + h->lay.why);
-    ResidentPlan plan;
-    cmd::ResidentArgs a{};
-    if (int rc = launch_resident(h, a, nullptr, nullptr, nullptr, nullptr, 0, h->stream, &plan)) return rc;
-    info[3] = plan.threads;
-    info[4] = plan.cpt;
-    info[5] = (int64_t)plan.smem;
+    const int vi = pick_variant(h);
+    if (vi < 0) return no_instance(h->lay);
+    const Variant& V = kVariants[vi];
+    info[3] = ((h->lay.G + V.CPT - 1) / V.CPT + 31) / 32 * 32;
+    info[4] = V.CPT;
+    info[5] = (int64_t)resident_smem(h->lay.NA, h->lay.G);
+    return CMD_OK;
+}
+
+int cmd_variant_count(void) { return kNumVariants; }
+
+int cmd_variant_info(cmd_handle* h, int32_t idx, char* name, int32_t name_len, int32_t* fits) {
+    cmd::clear_error();
+    if (idx < 0 || idx >= kNumVariants) return fail(CMD_ERR_INVALID_ARG, "variant index out of range");
+    if (name && name_len > 0) {
+        std::strncpy(name, kVariants[idx].name, (size_t)name_len - 1);
+        name[name_len - 1] = 0;
+    }
+    if (fits) *fits = (h && variant_fits(kVariants[idx], h->lay)) ? 1 : 0;
+    return CMD_OK;
+}
+
+int cmd_set_variant(cmd_handle* h, int32_t idx) {
+    cmd::clear_error();
+    if (int rc = check_handle(h, false)) return rc;
+    if (idx < -1 || idx >= kNumVariants) return fail(CMD_ERR_INVALID_ARG, "variant index out of range");
+    if (idx >= 0 && !variant_fits(kVariants[idx], h->lay))
+        return fail(CMD_ERR_UNSUPPORTED, "variant does not fit this lattice");
+    h->variant = idx;
+    return CMD_OK;
+}
+
+int cmd_get_variant(cmd_handle* h, int32_t* idx) {
+    cmd::clear_error();
+    if (int rc = check_handle(h, false)) return rc;
+    if (!idx) return fail(CMD_ERR_INVALID_ARG, "NULL output");
+    *idx = pick_variant(h);
+    return CMD_OK;
+}
+
+// Times every fitting variant on a B-trajectory, n_steps-step RK4 batch from the
+// handle's current state (observables every step, no drive) and keeps the
+// fastest.  ms[kNumVariants] (may be NULL) gets the times, -1 for variants that
+// do not fit.
+int cmd_autotune(cmd_handle* h, int64_t B, int64_t n_steps, int32_t* best, double* ms) {
+    cmd::clear_error();
+    if (int rc = check_handle(h, true)) return rc;
+    if (B <= 0 || n_steps <= 0) return fail(CMD_ERR_INVALID_ARG, "bad autotune size");
+    const int64_t rows = rows_for(n_steps, 1);
+    if (int rc = h->tune_obs.ensure((size_t)B * rows * 10 * sizeof(double))) return rc;
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    int win = -1;
+    float best_ms = 0.0f;
+    int rc = CMD_OK;
+    for (int i = 0; i < kNumVariants && rc == CMD_OK; ++i) {
+        if (ms) ms[i] = -1.0;
+        if (!variant_fits(kVariants[i], h->lay)) continue;
+        RunSpec r;
+        r.B = B;
+        r.y0 = h->state.as<double>();
+        r.obs = h->tune_obs.as<double>();
+        r.dt = 0.01;
+        r.n_steps = n_steps;
+        r.save = 1;
+        r.n_sites = (double)h->N;
+        r.variant = i;
+        float t = 0.0f;
+        for (int rep = 0; rep < 2 && rc == CMD_OK; ++rep) {     // first run warms up
+            cudaEventRecord(e0, h->stream);
+            rc = run_resident(h, r, h->stream, nullptr);
+            cudaEventRecord(e1, h->stream);
+            if (rc == CMD_OK) rc = sync(h);
+            if (rc == CMD_OK) cudaEventElapsedTime(&t, e0, e1);
+        }
+        if (rc != CMD_OK) break;
+        if (ms) ms[i] = t;
+        if (win < 0 || t < best_ms) { win = i; best_ms = t; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != CMD_OK) return rc;
+    if (win < 0) return no_instance(h->lay);
+    h->variant = win;
+    if (best) *best = win;
     return CMD_OK;
 }
 
@@ -781,9 +975,8 @@ int cmd_integrate_batched(cmd_handle* h, const double* init, const double* tau2,
     if (max_rows < rows) return fail(CMD_ERR_INVALID_ARG, "max_rows too small");
     std::vector<double> t1(B, h->t1), a(B, h->amp), obs((size_t)B * rows * 10);
     // Frames / AFM signs of the call override the lattice's for the observables.
-    std::vector<double> saved_frames = h->frames, saved_afm = h->afm;
-    if (frames) h->frames.assign(frames, frames + 9 * h->NA);
-    if (afm_signs) h->afm.assign(afm_signs, afm_signs + h->NA);
+    if (int rc = upload_frames(h, frames ? frames : h->frames.data(), afm_signs ? afm_signs : h->afm.data()))
+        return rc;
     cmd_batch_desc d{};
     d.B = B;
     d.states = init;
@@ -797,9 +990,9 @@ int cmd_integrate_batched(cmd_handle* h, const double* init, const double* tau2,
     d.obs = obs.data();
     d.final_states = nullptr;
     const int rc = cmd_run_batch(h, &d);
-    h->frames.swap(saved_frames);
-    h->afm.swap(saved_afm);
+    const int rc2 = upload_frames(h, h->frames.data(), h->afm.data());
     if (rc != CMD_OK) return rc;
+    if (rc2 != CMD_OK) return rc2;
     if (times) {
         int64_t r = 0;
         for (int64_t k = 0; k < n; k += save_interval) times[r++] = grid[k];

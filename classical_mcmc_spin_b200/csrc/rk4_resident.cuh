@@ -9,22 +9,27 @@
 // y += dt/6 (k1 + 2 k2 + 2 k3 + k4).
 //
 // Layout on chip (B200: 227 KB shared memory and 64K registers per CTA):
-//   * one thread owns CPT groups (unit cells) of NAT sites; y_n, the RK
-//     accumulator and its own current stage input stay in registers;
+//   * one thread owns CPT groups (unit cells) of NAT sites; y_n and the RK
+//     accumulator stay in registers for the whole trajectory (and, with YREG,
+//     the thread's own current stage input too);
 //   * the stage input every neighbour needs is published in shared memory,
 //     double buffered, class-major SoA: buf[(atom*3 + comp)*G + group], so a
 //     warp's 32 consecutive groups hit 32 consecutive doubles;
 //   * bonds whose partner lives in the thread's own cell ("local" slots,
-//     partner atom (a+1+n) % NAT) are read from registers, all others from
-//     shared memory through per-thread int32 offsets loaded once;
+//     partner atom (a+1+n) % NAT) never touch shared memory; all others are
+//     read through per-thread int32 offsets loaded once;
 //   * the coupling matrices are identical for every cell (checked on the host),
 //     so they are kernel parameters: compile-time-indexed constant-bank
 //     operands of the DFMAs, no loads at all.
-// One __syncthreads per stage.  The observables of step n (M_af, M_local,
-// M_global and E) come out of stage 0 of step n (E = 1/2 sum_i S_i.(H_i - B_i)
-// from the static field of that stage), are warp-reduced with a butterfly that
-// moves NV values in ~NV+log2(32/NV) shuffles, and are finished by one warp
-// after the next barrier.  No atomics: every sum has a fixed order.
+// One __syncthreads per stage, and nothing serial sits in front of it:
+//   * the pulse envelopes of every stage time come from a table filled by a
+//     parallel pre-pass (drive_table_kernel), loaded one step ahead;
+//   * the per-step observables leave as raw sums (sum of S per atom class and
+//     sum_i S_i.(H_i - B_i) over the static field of stage 0), warp-reduced
+//     with a butterfly that moves NV values in ~NV+log2(32/NV) shuffles and
+//     finished in parallel (warp q sums value q over the warps); a post-pass
+//     (finish_rows_kernel) applies the frames and the 1/N.
+// No atomics: every sum has a fixed order.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -37,8 +42,6 @@ struct Couplings {
     double J[NAT][Z][9];      // slot-ordered, local slots first
     double field[NAT][3];
     double onsite[NAT][9];
-    double frame[NAT][9];
-    double afm[NAT];
     double d1[NAT][3];        // pulse directions (frame-rotated)
     double d2[NAT][3];
     int zc[NAT];              // slots in use per class (<= Z)
@@ -52,21 +55,18 @@ struct Pulse {
 
 struct ResidentArgs {
     int G;                    // groups (cells) per trajectory
-    int nonlocal;             // offsets per (group, atom) in nbr
     long long n_steps;
     long long save_every;
     double T0, dt;
-    double inv_n;             // unused (kept for ABI of the launch struct)
-    double n_sites;           // N as a double (observables are divided by N)
-    const int* nbr;           // [G][NAT][nonlocal]
+    const int* nbr;           // [G][NAT][Z-LZ]
     const double* y0;         // [B or 1][N*3]
     long long y0_stride;      // doubles between trajectories (0: shared)
     double* y_out;            // [B][N*3] or nullptr
-    double* obs;              // [B][rows][10] or nullptr
+    double* raw;              // [B][rows][raw_stride] raw observable sums, or nullptr
+    long long raw_stride;     // doubles per raw row (>= 3*NAT+1)
     long long rows;           // rows per trajectory
     double* traj;             // [B][rows][N*3] or nullptr
-    const Pulse* pulses;      // [B] or nullptr
-    double width, freq;
+    const double* drive;      // [B][n_steps][6] envelope table, or nullptr (no drive)
 };
 
 constexpr int kRedStride = 16;  // doubles per warp in the reduction scratch
@@ -96,7 +96,7 @@ __device__ __forceinline__ double warp_reduce_many(double (&v)[NV]) {
 
 template <int NAT>
 struct NVals {
-    static constexpr int used = 3 * NAT + 1;
+    static constexpr int used = 3 * NAT + 1;      // sum S per atom class, then sum S.(H-B)
     static constexpr int value = used <= 4 ? 4 : (used <= 8 ? 8 : (used <= 16 ? 16 : 32));
 };
 
@@ -106,67 +106,119 @@ __device__ __forceinline__ double drive_factor(double amp, double x, double widt
     return amp * exp(-(u * u)) * cos(freq * x);
 }
 
-template <int NAT, int Z, int LZ, int CPT, int MAXT>
-__global__ void __launch_bounds__(MAXT, 1)
+// Envelope table [B][n_steps][6]: for each step n the factors (pulse 1, pulse 2)
+// at t_n, t_n + dt/2 and t_n + dt, t_n the accumulated time of the reference loop.
+__global__ void drive_table_kernel(const Pulse* __restrict__ pulses, const double* __restrict__ times,
+                                   long long n_steps, double dt, double width, double freq, long long B,
+                                   double* __restrict__ out) {
+    const long long total = B * n_steps * 6;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const long long b = e / (n_steps * 6);
+        const long long r = e - b * n_steps * 6;
+        const long long n = r / 6;
+        const int q = (int)(r - n * 6);
+        const double t = times[n];
+        const double tt = q < 2 ? t : (q < 4 ? t + 0.5 * dt : t + dt);
+        const Pulse p = pulses[b];
+        out[e] = (q & 1) ? drive_factor(p.a2, tt - p.t2, width, freq)
+                         : drive_factor(p.a1, tt - p.t1, width, freq);
+    }
+}
+
+// Raw sums -> {M_af[3], M_local[3], M_global[3], E/N} rows.  `raw` may alias
+// `obs` (raw_stride 10): each row is read completely before it is written.
+template <int NAT>
+__global__ void finish_rows_kernel(const double* raw, long long raw_stride, long long n_rows_total,
+                                   const double* __restrict__ frames, const double* __restrict__ afm,
+                                   double n_sites, double* obs) {
+    constexpr int NR = 3 * NAT + 1;
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n_rows_total;
+         r += (long long)gridDim.x * blockDim.x) {
+        double m[NR];
+#pragma unroll
+        for (int q = 0; q < NR; ++q) m[q] = raw[r * raw_stride + q];
+        double ml[3] = {0, 0, 0}, mg[3] = {0, 0, 0}, ma[3] = {0, 0, 0};
+#pragma unroll
+        for (int at = 0; at < NAT; ++at) {
+            const double* R = frames + 9 * at;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                ml[d] += m[3 * at + d];
+                const double v = R[3 * d] * m[3 * at] + R[3 * d + 1] * m[3 * at + 1] + R[3 * d + 2] * m[3 * at + 2];
+                mg[d] += v;
+                ma[d] += afm[at] * v;
+            }
+        }
+        double* o = obs + r * 10;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            o[d] = ma[d] / n_sites;
+            o[3 + d] = ml[d] / n_sites;
+            o[6 + d] = mg[d] / n_sites;
+        }
+        o[9] = 0.5 * m[3 * NAT] / n_sites;
+    }
+}
+
+template <int NAT, int Z, int LZ, int CPT, int MAXT, int MINB, bool YREG>
+__global__ void __launch_bounds__(MAXT, MINB)
 rk4_resident_kernel(const __grid_constant__ Couplings<NAT, Z> cp,
                     const __grid_constant__ ResidentArgs a) {
     constexpr int NL = Z - LZ;                       // non-local slots per atom
     constexpr int NV = NVals<NAT>::value;
+    constexpr int NR = NVals<NAT>::used;
     extern __shared__ double smem[];
     const int G = a.G;
     const int SB = NAT * 3 * G;                      // one stage buffer
-    double* bufA = smem;
-    double* bufB = smem + SB;
-    double* red = bufB + SB;                         // [32][kRedStride]
-    double* fin = red + 32 * kRedStride;             // [16] final-combine scratch
-    double* drv = fin + 16;                          // [2][6] drive factors
+    // Shared memory is addressed through 32-bit offsets (stage buffers at 0
+    // and SB), which keeps the addressing in the shared window and in 32-bit
+    // registers.
+    double* red = smem + 2 * SB;                     // [32][kRedStride]
+    double* drv = red + 32 * kRedStride;             // [2][6] envelopes of the current / next step
 
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
     const long long b = blockIdx.x;
 
-    double y[CPT][NAT][3], acc[CPT][NAT][3], yc[CPT][NAT][3];
+    double y[CPT][NAT][3], acc[CPT][NAT][3];
+    double yc[YREG ? CPT : 1][NAT][3];
     int nb[CPT][NAT][NL > 0 ? NL : 1];
-    bool own[CPT];
 
     const double* y0 = a.y0 + b * a.y0_stride;
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
         const int g = tid + k * blockDim.x;
-        own[k] = g < G;
+        const bool own = g < G;
 #pragma unroll
         for (int at = 0; at < NAT; ++at) {
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                const double v = own[k] ? y0[((long long)g * NAT + at) * 3 + c] : 0.0;
+                const double v = own ? y0[((long long)g * NAT + at) * 3 + c] : 0.0;
                 y[k][at][c] = v;
-                yc[k][at][c] = v;
+                if (YREG) yc[YREG ? k : 0][at][c] = v;
                 acc[k][at][c] = 0.0;
-                if (own[k]) bufA[(at * 3 + c) * G + g] = v;
+                if (own) smem[(at * 3 + c) * G + g] = v;
             }
 #pragma unroll
             for (int m = 0; m < NL; ++m)
-                nb[k][at][m] = own[k] ? a.nbr[((long long)g * NAT + at) * NL + m] : 0;
+                nb[k][at][m] = own ? a.nbr[((long long)g * NAT + at) * NL + m] : 0;
         }
     }
 
-    Pulse pl{0.0, 0.0, 0.0, 0.0};
-    if (a.pulses) pl = a.pulses[b];
-    const bool drive_on = a.pulses != nullptr && (pl.a1 != 0.0 || pl.a2 != 0.0);
+    const bool drive_on = a.drive != nullptr;
+    const double* dtab = drive_on ? a.drive + b * a.n_steps * 6 : nullptr;
     const double dt = a.dt;
-    double t = a.T0;
-
-    // drive factors for step 0: lanes 0..5 of the last warp
-    if (drive_on && warp == nwarps - 1 && lane < 6) {
-        const double tt = t + (lane < 2 ? 0.0 : (lane < 4 ? 0.5 * dt : dt));
-        drv[lane] = (lane & 1) ? drive_factor(pl.a2, tt - pl.t2, a.width, a.freq)
-                               : drive_factor(pl.a1, tt - pl.t1, a.width, a.freq);
-    }
+    // Lanes 0..5 of warp 0 stage the envelopes: loaded during stage 0 of step n
+    // for step n+1, stored to drv[] during stage 2, read by everyone after the
+    // stage-3 barrier.  Nothing waits on the global load.
+    const bool stager = drive_on && warp == 0 && lane < 6;
+    if (stager && a.n_steps > 0) drv[lane] = dtab[lane];
     __syncthreads();
 
-    // Field at the current stage input for (k, at); returns static field in Hs.
-    auto field_at = [&](const double* in, int k, int at, double (&H)[3]) {
-        const double S0 = yc[k][at][0], S1 = yc[k][at][1], S2 = yc[k][at][2];
+    // Static field at the current stage input of cell k, atom at.  S[][] holds
+    // the cell's NAT stage-input spins.
+    auto field_at = [&](int in, int k, int at, const double (&S)[NAT][3], double (&H)[3]) {
         if (cp.has_field) {
             H[0] = -cp.field[at][0]; H[1] = -cp.field[at][1]; H[2] = -cp.field[at][2];
         } else {
@@ -175,69 +227,56 @@ rk4_resident_kernel(const __grid_constant__ Couplings<NAT, Z> cp,
         if (cp.has_onsite) {
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
-                H[d] += 2.0 * cp.onsite[at][3 * d + 0] * S0;
-                H[d] += 2.0 * cp.onsite[at][3 * d + 1] * S1;
-                H[d] += 2.0 * cp.onsite[at][3 * d + 2] * S2;
+                H[d] += 2.0 * cp.onsite[at][3 * d + 0] * S[at][0];
+                H[d] += 2.0 * cp.onsite[at][3 * d + 1] * S[at][1];
+                H[d] += 2.0 * cp.onsite[at][3 * d + 2] * S[at][2];
             }
         }
 #pragma unroll
         for (int n = 0; n < LZ; ++n) {
             const int pb = (at + 1 + n) % NAT;
-            const double P0 = yc[k][pb][0], P1 = yc[k][pb][1], P2 = yc[k][pb][2];
 #pragma unroll
             for (int d = 0; d < 3; ++d)
-                H[d] += cp.J[at][n][3 * d] * P0 + cp.J[at][n][3 * d + 1] * P1 + cp.J[at][n][3 * d + 2] * P2;
+                H[d] += cp.J[at][n][3 * d] * S[pb][0] + cp.J[at][n][3 * d + 1] * S[pb][1] +
+                        cp.J[at][n][3 * d + 2] * S[pb][2];
         }
 #pragma unroll
         for (int m = 0; m < NL; ++m) {
             const int n = LZ + m;
             if (n < cp.zc[at]) {
-                const double* p = in + nb[k][at][m];
-                const double P0 = p[0], P1 = p[G], P2 = p[2 * G];
+                const int p = in + nb[k][at][m];
+                const double P0 = smem[p], P1 = smem[p + G], P2 = smem[p + 2 * G];
 #pragma unroll
                 for (int d = 0; d < 3; ++d)
                     H[d] += cp.J[at][n][3 * d] * P0 + cp.J[at][n][3 * d + 1] * P1 + cp.J[at][n][3 * d + 2] * P2;
             }
         }
     };
-
-    // Per-thread observable partials -> per-warp totals in red[warp][*].
+    auto load_cell = [&](int in, int k, double (&S)[NAT][3]) {
+        const int g = tid + k * blockDim.x;
+#pragma unroll
+        for (int at = 0; at < NAT; ++at)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                if (YREG) S[at][c] = yc[YREG ? k : 0][at][c];
+                else S[at][c] = smem[in + (at * 3 + c) * G + g];
+            }
+    };
+    // Per-thread partials -> per-warp totals in red[warp][*].
     auto reduce_partials = [&](double (&part)[NV]) {
         const double r = warp_reduce_many<NV>(part);
         constexpr int span = 32 / NV;
         if ((lane % span) == 0) red[warp * kRedStride + lane / span] = r;
     };
-    // One warp sums the per-warp totals and writes the 10-double row.
-    auto finish_row = [&](long long row) {
-        if (warp != 0) return;
-        constexpr int used = NVals<NAT>::used;
-        double s = 0.0;
-        if (lane < used)
-            for (int w = 0; w < nwarps; ++w) s += red[w * kRedStride + lane];
-        if (lane < used) fin[lane] = s;
-        __syncwarp();
-        if (lane == 0 && a.obs) {
-            double ml[3] = {0, 0, 0}, mg[3] = {0, 0, 0}, ma[3] = {0, 0, 0};
+    // Warp q sums value q (q = warp, warp + nwarps, ...) over the warps and
+    // writes it (runs after a barrier).
+    auto finish_raw = [&](long long row) {
+        if (a.raw == nullptr) return;
+        for (int q = warp; q < NR; q += nwarps) {
+            double s = lane < nwarps ? red[lane * kRedStride + q] : 0.0;
 #pragma unroll
-            for (int at = 0; at < NAT; ++at) {
-                const double m0 = fin[3 * at], m1 = fin[3 * at + 1], m2 = fin[3 * at + 2];
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    ml[d] += fin[3 * at + d];
-                    const double r = cp.frame[at][3 * d] * m0 + cp.frame[at][3 * d + 1] * m1 +
-                                     cp.frame[at][3 * d + 2] * m2;
-                    mg[d] += r;
-                    ma[d] += cp.afm[at] * r;
-                }
-            }
-            double* o = a.obs + (b * a.rows + row) * 10;
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                o[d] = ma[d] / a.n_sites;
-                o[3 + d] = ml[d] / a.n_sites;
-                o[6 + d] = mg[d] / a.n_sites;
-            }
-            o[9] = 0.5 * fin[3 * NAT] / a.n_sites;
+            for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) a.raw[(b * a.rows + row) * a.raw_stride + q] = s;
         }
     };
     auto write_traj = [&](long long row) {
@@ -245,8 +284,8 @@ rk4_resident_kernel(const __grid_constant__ Couplings<NAT, Z> cp,
         double* dst = a.traj + (b * a.rows + row) * (long long)G * NAT * 3;
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
-            if (!own[k]) continue;
             const int g = tid + k * blockDim.x;
+            if (g >= G) continue;
 #pragma unroll
             for (int at = 0; at < NAT; ++at)
 #pragma unroll
@@ -255,98 +294,91 @@ rk4_resident_kernel(const __grid_constant__ Couplings<NAT, Z> cp,
     };
 
     long long row = 0;
-    bool pending = false;       // a row's per-warp totals wait in red[]
-    double* in = bufA;
-    double* out = bufB;
+    long long save_left = 0;            // steps until the next saved row
+    bool pending = false;
+    int in = 0;          // offset of the buffer holding the current stage input
+    int out = SB;
     for (long long step = 0; step < a.n_steps; ++step) {
-        const bool observe = (step % a.save_every) == 0;
+        const bool observe = save_left == 0;
+        save_left = observe ? a.save_every - 1 : save_left - 1;
         const double* dv = drv + 6 * (step & 1);
+        double next_f = 0.0;
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
-            double f1 = 0.0, f2 = 0.0;
-            if (drive_on) {
-                const int ti = s == 0 ? 0 : (s == 3 ? 2 : 1);
-                f1 = dv[2 * ti];
-                f2 = dv[2 * ti + 1];
-            }
+            if (s == 0 && stager && step + 1 < a.n_steps) next_f = dtab[(step + 1) * 6 + lane];
+            if (s == 2 && stager && step + 1 < a.n_steps) drv[6 * ((step + 1) & 1) + lane] = next_f;
+            const int ti = s == 0 ? 0 : (s == 3 ? 2 : 1);
+            const double f1 = drive_on ? dv[2 * ti] : 0.0;
+            const double f2 = drive_on ? dv[2 * ti + 1] : 0.0;
+            const bool drive_now = drive_on && (f1 != 0.0 || f2 != 0.0);   // 0*d adds exactly 0
             double part[NV];
 #pragma unroll
             for (int q = 0; q < NV; ++q) part[q] = 0.0;
 #pragma unroll
             for (int k = 0; k < CPT; ++k) {
-                if (!own[k]) continue;
                 const int g = tid + k * blockDim.x;
-                double nx[NAT][3];
+                if (g >= G) continue;
+                double S[NAT][3];
+                load_cell(in, k, S);
+                double nx[YREG ? NAT : 1][3];
 #pragma unroll
                 for (int at = 0; at < NAT; ++at) {
                     double H[3];
-                    field_at(in, k, at, H);
-                    const double S0 = yc[k][at][0], S1 = yc[k][at][1], S2 = yc[k][at][2];
+                    field_at(in, k, at, S, H);
                     if (s == 0 && observe) {
-                        part[3 * at] += S0; part[3 * at + 1] += S1; part[3 * at + 2] += S2;
-                        part[3 * NAT] += S0 * (H[0] - cp.field[at][0]) + S1 * (H[1] - cp.field[at][1]) +
-                                         S2 * (H[2] - cp.field[at][2]);
+                        part[3 * at] += S[at][0]; part[3 * at + 1] += S[at][1]; part[3 * at + 2] += S[at][2];
+                        part[3 * NAT] += S[at][0] * (H[0] - cp.field[at][0]) + S[at][1] * (H[1] - cp.field[at][1]) +
+                                         S[at][2] * (H[2] - cp.field[at][2]);
                     }
-                    if (drive_on) {
+                    if (drive_now) {
 #pragma unroll
                         for (int d = 0; d < 3; ++d) H[d] -= cp.d1[at][d] * f1 + cp.d2[at][d] * f2;
                     }
-                    const double k0 = H[1] * S2 - H[2] * S1;
-                    const double k1 = H[2] * S0 - H[0] * S2;
-                    const double k2 = H[0] * S1 - H[1] * S0;
-                    const double kk[3] = {k0, k1, k2};
+                    const double kk[3] = {H[1] * S[at][2] - H[2] * S[at][1], H[2] * S[at][0] - H[0] * S[at][2],
+                                          H[0] * S[at][1] - H[1] * S[at][0]};
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
+                        double v;
                         if (s == 0) {
                             acc[k][at][c] = kk[c];
-                            nx[at][c] = 1.0 * y[k][at][c] + (0.5 * dt) * kk[c];
+                            v = 1.0 * y[k][at][c] + (0.5 * dt) * kk[c];
                         } else if (s == 1) {
                             acc[k][at][c] = acc[k][at][c] + 2.0 * kk[c];
-                            nx[at][c] = 1.0 * y[k][at][c] + (0.5 * dt) * kk[c];
+                            v = 1.0 * y[k][at][c] + (0.5 * dt) * kk[c];
                         } else if (s == 2) {
                             acc[k][at][c] = acc[k][at][c] + 2.0 * kk[c];
-                            nx[at][c] = 1.0 * y[k][at][c] + dt * kk[c];
+                            v = 1.0 * y[k][at][c] + dt * kk[c];
                         } else {
                             y[k][at][c] += (dt / 6.0) * (acc[k][at][c] + kk[c]);
-                            nx[at][c] = y[k][at][c];
+                            v = y[k][at][c];
                         }
+                        if (YREG) nx[YREG ? at : 0][c] = v;     // own registers change after the cell
+                        else smem[out + (at * 3 + c) * G + g] = v;
                     }
                 }
+                if (YREG) {
 #pragma unroll
-                for (int at = 0; at < NAT; ++at)
+                    for (int at = 0; at < NAT; ++at)
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        yc[k][at][c] = nx[at][c];
-                        out[(at * 3 + c) * G + g] = nx[at][c];
-                    }
+                        for (int c = 0; c < 3; ++c) {
+                            yc[YREG ? k : 0][at][c] = nx[YREG ? at : 0][c];
+                            smem[out + (at * 3 + c) * G + g] = nx[YREG ? at : 0][c];
+                        }
+                }
             }
             if (s == 0 && observe) {
                 write_traj(row);
                 reduce_partials(part);
             }
             if (s == 1 && pending) {
-                finish_row(row);
+                finish_raw(row);
                 ++row;
                 pending = false;
             }
-            if (s == 3 && drive_on && warp == nwarps - 1 && lane < 6) {
-                const double tn = t + dt;
-                const double tt = tn + (lane < 2 ? 0.0 : (lane < 4 ? 0.5 * dt : dt));
-                drv[6 * ((step + 1) & 1) + lane] =
-                    (lane & 1) ? drive_factor(pl.a2, tt - pl.t2, a.width, a.freq)
-                               : drive_factor(pl.a1, tt - pl.t1, a.width, a.freq);
-            }
             __syncthreads();
             if (s == 0 && observe) pending = true;
-            double* tmp = in; in = out; out = tmp;
+            const int tmp = in; in = out; out = tmp;
         }
-        t += dt;
-    }
-    if (pending) {          // defensive: stage 1 always follows stage 0 inside a step
-        finish_row(row);
-        ++row;
-        pending = false;
-        __syncthreads();
     }
     // Final observation of y(t_end): one more static-field evaluation for E.
     {
@@ -355,28 +387,30 @@ rk4_resident_kernel(const __grid_constant__ Couplings<NAT, Z> cp,
         for (int q = 0; q < NV; ++q) part[q] = 0.0;
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
-            if (!own[k]) continue;
+            const int g = tid + k * blockDim.x;
+            if (g >= G) continue;
+            double S[NAT][3];
+            load_cell(in, k, S);
 #pragma unroll
             for (int at = 0; at < NAT; ++at) {
                 double H[3];
-                field_at(in, k, at, H);
-                const double S0 = yc[k][at][0], S1 = yc[k][at][1], S2 = yc[k][at][2];
-                part[3 * at] += S0; part[3 * at + 1] += S1; part[3 * at + 2] += S2;
-                part[3 * NAT] += S0 * (H[0] - cp.field[at][0]) + S1 * (H[1] - cp.field[at][1]) +
-                                 S2 * (H[2] - cp.field[at][2]);
+                field_at(in, k, at, S, H);
+                part[3 * at] += S[at][0]; part[3 * at + 1] += S[at][1]; part[3 * at + 2] += S[at][2];
+                part[3 * NAT] += S[at][0] * (H[0] - cp.field[at][0]) + S[at][1] * (H[1] - cp.field[at][1]) +
+                                 S[at][2] * (H[2] - cp.field[at][2]);
             }
         }
         write_traj(row);
         reduce_partials(part);
         __syncthreads();
-        finish_row(row);
+        finish_raw(row);
     }
     if (a.y_out) {
         double* dst = a.y_out + b * (long long)G * NAT * 3;
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
-            if (!own[k]) continue;
             const int g = tid + k * blockDim.x;
+            if (g >= G) continue;
 #pragma unroll
             for (int at = 0; at < NAT; ++at)
 #pragma unroll

@@ -48,6 +48,33 @@ class GPULatticeDataHandle:
         except Exception:
             pass
 
+    def variants(self) -> list:
+        """[(index, name, fits this lattice)] of the resident-kernel variants."""
+        L = nat.lib()
+        out = []
+        for i in range(L.cmd_variant_count()):
+            buf = C.create_string_buffer(128)
+            fits = C.c_int32()
+            check(L.cmd_variant_info(self.ptr, i, buf, 128, C.byref(fits)), "cmd_variant_info")
+            out.append((i, buf.value.decode(), bool(fits.value)))
+        return out
+
+    def set_variant(self, idx: int) -> None:
+        check(nat.lib().cmd_set_variant(self.ptr, int(idx)), "cmd_set_variant")
+
+    def get_variant(self) -> int:
+        v = C.c_int32()
+        check(nat.lib().cmd_get_variant(self.ptr, C.byref(v)), "cmd_get_variant")
+        return v.value
+
+    def autotune(self, B: int, n_steps: int) -> tuple:
+        """Times every fitting variant; pins and returns (best index, ms per variant)."""
+        n = nat.lib().cmd_variant_count()
+        ms = np.zeros(n)
+        best = C.c_int32()
+        check(nat.lib().cmd_autotune(self.ptr, int(B), int(n_steps), C.byref(best), dptr(ms)), "cmd_autotune")
+        return best.value, ms
+
     def layout_info(self) -> dict:
         info = np.zeros(6, np.int64)
         check(nat.lib().cmd_layout_info(self.ptr, iptr(info)), "cmd_layout_info")

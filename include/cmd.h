@@ -186,6 +186,25 @@ int cmd_run_batch_device(cmd_handle* h, const cmd_batch_desc* d, void* stream, i
  * bytes per trajectory. */
 int cmd_layout_info(cmd_handle* h, int64_t* info);
 
+/*
+ * Autotuner over the resident-kernel variants compiled into the library
+ * (cells per thread x threads per CTA x CTAs per SM x own stage input kept in
+ * registers or re-read from shared memory).  No reference counterpart.
+ *   cmd_variant_count     number of variants in the library
+ *   cmd_variant_info      name of variant idx and whether it fits h's lattice
+ *   cmd_set_variant       pin a variant for h (-1: back to the default choice)
+ *   cmd_get_variant       variant h uses now
+ *   cmd_autotune          time every fitting variant on a B-trajectory,
+ *                         n_steps-step batch from h's current spins, pin the
+ *                         fastest; ms[cmd_variant_count()] gets the times
+ *                         (-1 for variants that do not fit), may be NULL
+ */
+int cmd_variant_count(void);
+int cmd_variant_info(cmd_handle* h, int32_t idx, char* name, int32_t name_len, int32_t* fits);
+int cmd_set_variant(cmd_handle* h, int32_t idx);
+int cmd_get_variant(cmd_handle* h, int32_t* idx);
+int cmd_autotune(cmd_handle* h, int64_t B, int64_t n_steps, int32_t* best, double* ms);
+
 /* Host-only version of the layout analysis cmd_create performs (no CUDA
  * call): fills info[0..5] like cmd_layout_info, info[6] = leading local slots
  * per atom; returns CMD_ERR_UNSUPPORTED with the reason when no resident

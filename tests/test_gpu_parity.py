@@ -68,10 +68,14 @@ def test_plain_rk4_matches_boost_form_oracle(api, oracle):
     h = lat.to_gpu()
     api.set_gpu_spins(h, s0)
     traj, obs, times = api.integrate_gpu(h, 0.0, 9.995, 0.01, 10, "rk4", with_states=True)
-    rows, fin = o.md_rk4(s0, 0.0, 9.995, 0.01, 10)
-    n = min(len(rows), len(obs))
-    assert np.abs(obs[:n, :9] - rows[:n, 1:10]).max() <= TOL_M
-    assert np.abs(traj[n - 1][1] - fin).max() <= TOL_S
+    # integrate_const stops at the last t0 + k dt <= T1 + eps, the GPU loop at
+    # the first t >= T1: T1 = 10.005 gives the same 1000 steps.
+    rows, fin = o.md_rk4(s0, 0.0, 10.005, 0.01, 10)
+    assert len(rows) == len(obs) == 101
+    np.testing.assert_allclose(times, rows[:, 0], rtol=0, atol=1e-12)
+    assert np.abs(obs[:, :9] - rows[:, 1:10]).max() <= TOL_M
+    assert np.abs(obs[:, 9] - rows[:, 10]).max() <= TOL_M
+    assert np.abs(traj[-1][1] - fin).max() <= TOL_S
 
 
 def test_driven_rk4_matches_oracle(api, oracle):
@@ -232,3 +236,41 @@ def test_errors_are_status_codes(api, native):
     with pytest.raises(CmdError) as e:
         api.step_gpu(big, 0.0, 0.01)
     assert e.value.code == native.CMD_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("kind", ["kitaev", "pyro"])
+def test_every_kernel_variant_matches_oracle(api, oracle, kind):
+    """Each resident-kernel variant that fits the lattice gives the oracle's trajectory."""
+    if kind == "kitaev":
+        lat, o = _pair(oracle, "kitaev", (24, 24, 1))
+    else:
+        lat, o = _pair(oracle, "pyro", (4, 4, 4), h=0.2, field_direction=R111, Jzz=1.0, Jpm=0.05, Jpmpm=0.02)
+    s0 = _spins(lat.lattice_size, 21)
+    fin = np.tile(R111, lat.N_atoms)
+    fd = lat.rotate_pulse(fin, fin)
+    o.set_pulse(fin, 0.1, fin, 0.6, 0.5, 0.5, 0.7)
+    rows, ofin = o.md_rk4(s0, -0.5, 1.495, 0.01, 5, gpu_loop=True)
+    h = lat.to_gpu()
+    fits = [i for i, _, f in h.variants() if f]
+    assert fits
+    for v in fits:
+        h.set_variant(v)
+        assert h.get_variant() == v
+        api.set_gpu_spins(h, s0)
+        api.set_gpu_pulse(h, fd, 0.5, 0.5, 0.7, 0.1, 0.6)
+        _, obs, times = api.integrate_gpu(h, -0.5, 1.495, 0.01, 5, "rk4", with_states=False)
+        assert len(obs) == len(rows), v
+        assert np.abs(obs[:, :9] - rows[:, 1:10]).max() <= TOL_M, v
+        assert np.abs(obs[:, 9] - rows[:, 10]).max() <= TOL_M, v
+        assert np.abs(api.get_gpu_spins(h) - ofin).max() <= TOL_S, v
+
+
+def test_autotune_picks_a_fitting_variant(api, oracle):
+    lat, o = _pair(oracle, "kitaev", (8, 8, 1))
+    h = lat.to_gpu()
+    api.set_gpu_spins(h, _spins(lat.lattice_size, 3))
+    best, ms = h.autotune(16, 20)
+    fits = {i for i, _, f in h.variants() if f}
+    assert best in fits and ms[best] > 0
+    assert all((ms[i] > 0) == (i in fits) for i in range(len(ms)))
+    assert h.get_variant() == best

@@ -128,17 +128,31 @@ def _golden(name):
     return np.load(p)
 
 
-def test_oracle_matches_reference_gpu_rk4_golden(oracle):
-    """The reference's own GPU integrator (integrate_gpu, 'rk4') vs the oracle."""
-    g = _golden("ref_gpu_rk4_kitaev.npz")
-    L = oracle.OracleLattice.kitaev(int(g["d1"]), int(g["d2"]), 1)
+@pytest.mark.parametrize("name", ["ref_gpu_rk4_kitaev.npz", "ref_gpu_rk4_kitaev24.npz", "ref_gpu_rk4_pyrochlore.npz"])
+def test_oracle_matches_reference_gpu_rk4_golden(oracle, name):
+    """The reference's own GPU integrator (integrate_gpu, 'rk4') vs the oracle, saved states."""
+    g = _golden(name)
+    if "pyrochlore" in name:
+        R111 = np.ones(3) / np.sqrt(3.0)
+        L = oracle.OracleLattice.pyrochlore_nk(*[int(x) for x in g["dims"]], h=float(g["h"]), direction=R111,
+                                               Jzz=1.0, Jpm=0.05, Jpmpm=0.02)
+    else:
+        L = oracle.OracleLattice.kitaev(int(g["d1"]), int(g["d2"]), 1)
     s = g["init"].copy()
     save = int(g["save_interval"])
+    dt = float(g["dt"])
+    t = 0.0
+    steps = 0
     for r, t_ref in enumerate(g["times"]):
+        assert abs(t - t_ref) <= 1e-12
         assert np.abs(s - g["states"][r]).max() < 1e-12, r
         if r + 1 < len(g["times"]):
-            for k in range(save):
-                s = L.rk4_step(s, t_ref + k * float(g["dt"]), float(g["dt"]), gpu_form=True)
+            n = save if r + 2 < len(g["times"]) else int(round((g["times"][r + 1] - t_ref) / dt))
+            for k in range(n):
+                s = L.rk4_step(s, t, dt, gpu_form=True)
+                t += dt
+                steps += 1
+    assert steps > 0
 
 
 def test_oracle_matches_reference_gpu_driven_golden(oracle):
