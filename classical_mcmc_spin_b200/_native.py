@@ -49,6 +49,13 @@ class BatchDesc(C.Structure):
                 ("obs", C.c_void_p), ("final_states", C.c_void_p), ("pulse4", C.c_void_p)]
 
 
+class TrajSpec(C.Structure):
+    _fields_ = [("lattice", C.c_void_p), ("state", C.c_void_p), ("T0", C.c_double), ("T1", C.c_double),
+                ("dt", C.c_double), ("t1", C.c_double), ("t2", C.c_double), ("a1", C.c_double), ("a2", C.c_double),
+                ("rows", C.c_void_p), ("max_rows", C.c_int64), ("final_state", C.c_void_p),
+                ("stats", C.c_int64 * 4)]
+
+
 class CmdError(RuntimeError):
     def __init__(self, code: int, where: str, msg: str):
         super().__init__(f"{where}: {STATUS_NAMES.get(code, code)}: {msg}")
@@ -76,6 +83,7 @@ _SIGS = {
     "cmd_run_batch_device": (C.c_int, [C.c_void_p, C.POINTER(BatchDesc), C.c_void_p, _I32]),
     "cmd_layout_info": (C.c_int, [C.c_void_p, _I64]),
     "cmd_plan_layout": (C.c_int, [C.POINTER(LatticeDesc), _I64]),
+    "cmd_run_uneven": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.c_double, C.c_double, C.c_int64]),
     "cmd_variant_count": (C.c_int, []),
     "cmd_variant_info": (C.c_int, [C.c_void_p, C.c_int32, C.c_char_p, C.c_int32, _I32]),
     "cmd_set_variant": (C.c_int, [C.c_void_p, C.c_int32]),

@@ -12,6 +12,7 @@
 #include "cmd.h"
 #include "cmd_internal.h"
 #include "rk4_resident.cuh"
+#include "rk_global.cuh"
 
 #include <cuda_runtime.h>
 
@@ -89,7 +90,8 @@ struct DevBuf {
 
 struct cmd_handle {
     int64_t N = 0;
-    int NA = 0;
+    int NA = 0;                 // sites per group (classes) used by the kernels
+    int n_atoms_ref = 0;        // the caller's n_atoms when it differs from NA
     int zmax = 0;
     std::vector<double> field, onsite, frames, afm;   // per atom
     bool has_field = false, has_onsite = false;
@@ -97,6 +99,7 @@ struct cmd_handle {
     cudaStream_t stream = nullptr;
     DevBuf state, nbr, obs, traj, batch_states, batch_out, pulses, scratch;
     DevBuf dframes, dafm, times, drive, raw, tune_states, tune_obs;
+    DevBuf gwork, gmeta, gstat, grows, gqueue;
     bool has_state = false;
     int variant = -1;           // resident-kernel variant; -1 = heuristic default
     // pulse (set_gpu_pulse)
@@ -121,12 +124,24 @@ bool mat_zero(const double* a) {
 // field/onsite depend on the atom only, and after dropping all-zero coupling
 // entries (which add exactly 0.0) each site of atom a carries the same
 // multiset of (J, partner atom) as the site of atom a in cell 0.
-void analyse(const cmd_lattice_desc& d, Layout& L) {
+//
+// `NA` is the group size: n_atoms itself, or a divisor of it when a large unit
+// cell is a union of identical smaller groups (the 16-site cubic pyrochlore cell
+// = 4 FCC translations of the 4-site group).  Sites are then grouped as
+// consecutive runs of NA, and everything per atom must depend on atom % NA.
+void analyse_as(const cmd_lattice_desc& d, int NA, Layout& L) {
     L = Layout{};
     const int64_t N = d.lattice_size;
-    const int NA = d.n_atoms;
     const int zmax = d.max_bilinear;
     if (NA <= 0 || N % NA != 0) { L.why = "lattice_size is not a multiple of n_atoms"; return; }
+    if (d.n_atoms % NA != 0) { L.why = "group size does not divide n_atoms"; return; }
+    for (int a = NA; a < d.n_atoms; ++a) {
+        if ((d.frames && std::memcmp(d.frames + 9 * a, d.frames + 9 * (a % NA), 9 * sizeof(double)) != 0) ||
+            (d.afm_signs && d.afm_signs[a] != d.afm_signs[a % NA])) {
+            L.why = "sublattice frames differ within a group class";
+            return;
+        }
+    }
     L.NA = NA;
     L.G = N / NA;
     for (int64_t i = 0; i < N; ++i) {
@@ -176,6 +191,13 @@ void analyse(const cmd_lattice_desc& d, Layout& L) {
         } else {
             order = canon;
         }
+        // Non-local slots in a size-independent order (partner atom, then the
+        // coupling matrix), so lattices of one unit cell share one coupling table.
+        for (int a = 0; a < NA; ++a)
+            std::stable_sort(order[a].begin() + LZ, order[a].end(), [](const Slot& x, const Slot& y) {
+                if (x.b != y.b) return x.b < y.b;
+                return std::memcmp(x.J, y.J, 9 * sizeof(double)) < 0;
+            });
         int Z = 0;
         for (int a = 0; a < NA; ++a) Z = std::max(Z, (int)order[a].size());
         const int NL = Z - LZ;
@@ -235,6 +257,27 @@ void analyse(const cmd_lattice_desc& d, Layout& L) {
 }
 
 int64_t rows_for(int64_t n_steps, int64_t save) { return (n_steps + save - 1) / save + 1; }
+
+bool layout_has_kernel(const Layout& L);
+
+// Chooses the group size: the whole unit cell when a kernel covers it,
+// otherwise the largest of 4, 2, 1 dividing n_atoms that gives a uniform
+// layout some kernel covers.
+void analyse(const cmd_lattice_desc& d, Layout& L) {
+    analyse_as(d, d.n_atoms, L);
+    if (L.uniform && layout_has_kernel(L)) return;
+    Layout first = L;
+    for (int na : {4, 2, 1}) {
+        if (na >= d.n_atoms || d.n_atoms % na != 0) continue;
+        Layout alt;
+        analyse_as(d, na, alt);
+        if (alt.uniform && layout_has_kernel(alt)) {
+            L = std::move(alt);
+            return;
+        }
+    }
+    L = std::move(first);
+}
 
 template <int NAT, int Z>
 void fill_couplings(const cmd_handle* h, const double* d1, const double* d2, cmd::Couplings<NAT, Z>& cp) {
@@ -442,6 +485,139 @@ int run_resident(cmd_handle* h, const RunSpec& r, cudaStream_t st, int32_t* laun
     return CMD_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Global-state integrator (rk_global.cuh): controlled / fixed Dormand-Prince and
+// global-memory RK4, persistent over a queue of trajectories.
+
+// Unit-cell types compiled into rk_global_kernel: type 0 = 2-atom cells with 3
+// bonds per site (honeycomb), type 1 = 4-atom cells with 6 bonds per site
+// (nearest-neighbour pyrochlore).
+int global_type(const Layout& L) {
+    if (!L.uniform) return -1;
+    if (L.NA == 2 && L.Z == 3 && L.LZ == 1) return 0;
+    if (L.NA == 4 && L.Z == 6 && L.LZ == 3) return 1;
+    return -1;
+}
+
+bool layout_has_kernel(const Layout& L) { return default_variant(L) >= 0 || global_type(L) >= 0; }
+
+struct GJob {
+    cmd_handle* h = nullptr;
+    const double* y0 = nullptr;     // device AoS
+    double* yout = nullptr;         // device AoS or null
+    double* rows = nullptr;         // device [max_rows][11]
+    double* traj = nullptr;         // device [max_rows][N*3] or null
+    int64_t max_rows = 0;
+    double T0 = 0, T1 = 0, dt0 = 0;
+    int64_t n_steps = 0, save_every = 1;
+    cmd::Pulse pulse{0, 0, 0, 0};
+};
+
+bool same_couplings(const cmd_handle* a, const cmd_handle* b) {
+    return a->lay.J == b->lay.J && a->lay.zc == b->lay.zc && a->field == b->field && a->onsite == b->onsite &&
+           a->fd == b->fd && a->width == b->width && a->freq == b->freq && a->frames == b->frames &&
+           a->afm == b->afm;
+}
+
+int sync(cmd_handle* h);
+
+// Runs the jobs in one persistent launch on `owner`'s stream; stats [B][4] out.
+int run_global(cmd_handle* owner, std::vector<GJob>& jobs, int mode, double abs_tol, double rel_tol,
+               int64_t max_steps, std::vector<long long>& stats) {
+    const int64_t B = (int64_t)jobs.size();
+    if (B <= 0) return fail(CMD_ERR_INVALID_ARG, "empty batch");
+    const cmd_handle* src[2] = {nullptr, nullptr};
+    for (const GJob& j : jobs) {
+        const int ty = global_type(j.h->lay);
+        if (ty < 0) return no_instance(j.h->lay);
+        if (!src[ty]) src[ty] = j.h;
+        else if (!same_couplings(src[ty], j.h))
+            return fail(CMD_ERR_UNSUPPORTED, "lattices of one unit-cell type must share couplings and pulse settings");
+    }
+    if (src[0] && src[1] && (src[0]->width != src[1]->width || src[0]->freq != src[1]->freq))
+        return fail(CMD_ERR_UNSUPPORTED, "pulse width / frequency must agree across the batch");
+    // longest first (cells x expected steps)
+    std::vector<int64_t> order(B);
+    for (int64_t i = 0; i < B; ++i) order[i] = i;
+    auto cost = [&](int64_t i) {
+        const GJob& j = jobs[i];
+        const double steps = j.n_steps > 0 ? (double)j.n_steps : (j.T1 - j.T0) / std::max(j.dt0, 1e-300);
+        return (double)j.h->N * steps;
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) { return cost(x) > cost(y); });
+    size_t work_total = 0;
+    std::vector<size_t> woff(B);
+    for (int64_t i = 0; i < B; ++i) {
+        woff[i] = work_total;
+        work_total += (size_t)cmd::kGVectors * 3 * jobs[i].h->N;
+    }
+    if (int rc = owner->gwork.ensure(work_total * sizeof(double))) return rc;
+    if (int rc = owner->gmeta.ensure((size_t)B * sizeof(cmd::GTraj))) return rc;
+    if (int rc = owner->gstat.ensure((size_t)B * 4 * sizeof(long long))) return rc;
+    if (int rc = owner->gqueue.ensure(sizeof(int))) return rc;
+    std::vector<cmd::GTraj> tr(B);
+    long long* dstat = owner->gstat.as<long long>();
+    for (int64_t q = 0; q < B; ++q) {
+        const int64_t i = order[q];
+        const GJob& j = jobs[i];
+        cmd::GTraj& T = tr[q];
+        T.type = global_type(j.h->lay);
+        T.G = (int)j.h->lay.G;
+        T.nbr = j.h->nbr.as<int>();
+        T.y0 = j.y0;
+        T.yout = j.yout;
+        T.work = owner->gwork.as<double>() + woff[i];
+        T.rows = j.rows;
+        T.traj = j.traj;
+        T.max_rows = j.max_rows;
+        T.T0 = j.T0; T.T1 = j.T1; T.dt0 = j.dt0;
+        T.n_steps = j.n_steps;
+        T.save_every = j.save_every;
+        T.pulse = j.pulse;
+        T.stat = dstat + 4 * i;
+    }
+    cudaStream_t st = owner->stream;
+    CUDA_TRY(cudaMemcpyAsync(owner->gmeta.p, tr.data(), B * sizeof(cmd::GTraj), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemsetAsync(owner->gqueue.p, 0, sizeof(int), st));
+    CUDA_TRY(cudaMemsetAsync(owner->gstat.p, 0, B * 4 * sizeof(long long), st));
+    cmd::GArgs a{};
+    a.traj = owner->gmeta.as<cmd::GTraj>();
+    a.B = (int)B;
+    a.queue = owner->gqueue.as<int>();
+    a.mode = mode;
+    a.abs_tol = abs_tol;
+    a.rel_tol = rel_tol;
+    a.max_steps = max_steps;
+    const cmd_handle* any = src[0] ? src[0] : src[1];
+    a.width = any->width;
+    a.freq = any->freq;
+    cmd::Couplings<2, 3> c0;
+    cmd::Couplings<4, 6> c1;
+    std::memset(&c0, 0, sizeof(c0));
+    std::memset(&c1, 0, sizeof(c1));
+    if (src[0]) {
+        fill_couplings<2, 3>(src[0], src[0]->fd.data(), src[0]->fd.data() + 3 * src[0]->NA, c0);
+        a.frames0 = src[0]->dframes.as<double>();
+        a.afm0 = src[0]->dafm.as<double>();
+    }
+    if (src[1]) {
+        fill_couplings<4, 6>(src[1], src[1]->fd.data(), src[1]->fd.data() + 3 * src[1]->NA, c1);
+        a.frames1 = src[1]->dframes.as<double>();
+        a.afm1 = src[1]->dafm.as<double>();
+    }
+    auto kern = cmd::rk_global_kernel<2, 3, 1, 4, 6, 3>;
+    int dev = 0, nsm = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0);
+    const int grid = (int)std::min<int64_t>(B, (int64_t)nsm * std::max(per_sm, 1));
+    kern<<<grid, 256, 0, st>>>(c0, c1, a);
+    CUDA_TRY(cudaGetLastError());
+    stats.assign((size_t)B * 4, 0);
+    CUDA_TRY(cudaMemcpyAsync(stats.data(), owner->gstat.p, B * 4 * sizeof(long long), cudaMemcpyDeviceToHost, st));
+    return sync(owner);
+}
+
 // Reference GPU loop (integrator.cuh:477-483): number of steps and times.
 int64_t count_steps(double T0, double T1, double dt, double margin, std::vector<double>* times) {
     int64_t n = 0;
@@ -505,6 +681,19 @@ int upload_frames(cmd_handle* h, const double* frames, const double* afm) {
     return sync(h);
 }
 
+int caller_atoms(const cmd_handle* h) { return h->n_atoms_ref ? h->n_atoms_ref : h->NA; }
+
+// Per-atom array of the caller's unit cell [caller atoms][w] -> per class [NA][w].
+int reduce_per_class(const cmd_handle* h, const double* in, int w, std::vector<double>& out, const char* what) {
+    const int ca = caller_atoms(h);
+    out.assign(in, in + (size_t)w * h->NA);
+    for (int a = h->NA; a < ca; ++a)
+        for (int c = 0; c < w; ++c)
+            if (in[a * w + c] != out[(a % h->NA) * w + c])
+                return fail(CMD_ERR_UNSUPPORTED, std::string(what) + " must be uniform per sublattice class");
+    return CMD_OK;
+}
+
 int check_handle(cmd_handle* h, bool need_state) {
     if (!h) return fail(CMD_ERR_INVALID_ARG, "NULL handle");
     if (need_state && !h->has_state) return fail(CMD_ERR_STATE, "spins not set (call cmd_set_spins first)");
@@ -554,6 +743,17 @@ int cmd_create(const cmd_lattice_desc* d, cmd_handle** out) {
     for (double v : h->onsite) h->has_onsite |= (v != 0.0);
     h->fd.assign(2 * 3 * (size_t)d->n_atoms, 0.0);
     analyse(*d, h->lay);
+    if (h->lay.uniform && h->lay.NA != d->n_atoms) {
+        // grouped cell: per-class tables are the first NA atoms' (checked uniform)
+        const int na = h->lay.NA;
+        h->NA = na;
+        h->field.resize(3 * na);
+        h->onsite.resize(9 * na);
+        h->frames.resize(9 * na);
+        h->afm.resize(na);
+        h->fd.assign(6 * (size_t)na, 0.0);
+        h->n_atoms_ref = d->n_atoms;
+    }
     int rc = CMD_OK;
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
         rc = fail(CMD_ERR_CUDA, "cudaStreamCreate failed (no CUDA device?)");
@@ -578,7 +778,7 @@ int cmd_destroy(cmd_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (DevBuf* b : {&h->state, &h->nbr, &h->obs, &h->traj, &h->batch_states, &h->batch_out,
                       &h->pulses, &h->scratch, &h->dframes, &h->dafm, &h->times, &h->drive, &h->raw,
-                      &h->tune_states, &h->tune_obs})
+                      &h->tune_states, &h->tune_obs, &h->gwork, &h->gmeta, &h->gstat, &h->grows, &h->gqueue})
         b->release();
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -592,7 +792,18 @@ int cmd_set_pulse(cmd_handle* h, const double* fd, double amp, double width, dou
     if (!fd) return fail(CMD_ERR_INVALID_ARG, "NULL field_drive");
     if (!(width != 0.0) || !std::isfinite(amp) || !std::isfinite(width) || !std::isfinite(freq))
         return fail(CMD_ERR_INVALID_ARG, "bad pulse parameters");
-    h->fd.assign(fd, fd + 6 * (size_t)h->NA);
+    // field_drive is [2][caller atoms][3]; a grouped cell needs it uniform per class
+    const int ca = caller_atoms(h);
+    std::vector<double> v(6 * (size_t)h->NA);
+    for (int p = 0; p < 2; ++p)
+        for (int a = 0; a < ca; ++a)
+            for (int c = 0; c < 3; ++c) {
+                const double x = fd[(p * ca + a) * 3 + c];
+                if (a < h->NA) v[(p * h->NA + a) * 3 + c] = x;
+                else if (x != v[(p * h->NA + a % h->NA) * 3 + c])
+                    return fail(CMD_ERR_UNSUPPORTED, "pulse directions must be uniform per sublattice class");
+            }
+    h->fd.swap(v);
     h->amp = amp; h->width = width; h->freq = freq; h->t1 = t1; h->t2 = t2;
     return CMD_OK;
 }
@@ -664,36 +875,170 @@ int run_single(cmd_handle* h, double T0, double dt, int64_t n_steps, int64_t sav
 
 }  // namespace
 
+namespace {
+
+int mode_of(int method) {
+    return method == CMD_RK45 ? cmd::kModeRK45 : (method == CMD_DOPRI5_FIXED ? cmd::kModeDopri5Fixed : cmd::kModeRK4);
+}
+
+// One trajectory of the handle through the global-state integrator.
+int run_global_single(cmd_handle* h, int method, double T0, double T1, double dt, int64_t n_steps, int64_t save,
+                      int64_t max_rows, bool want_traj, int64_t* rows_needed) {
+    GJob j;
+    j.h = h;
+    j.y0 = h->state.as<double>();
+    j.yout = h->state.as<double>();
+    if (int rc = h->grows.ensure((size_t)std::max<int64_t>(max_rows, 1) * 11 * sizeof(double))) return rc;
+    j.rows = h->grows.as<double>();
+    if (want_traj) {
+        if (int rc = h->traj.ensure((size_t)std::max<int64_t>(max_rows, 1) * h->N * 3 * sizeof(double))) return rc;
+        j.traj = h->traj.as<double>();
+    }
+    j.max_rows = max_rows;
+    j.T0 = T0; j.T1 = T1; j.dt0 = dt;
+    j.n_steps = n_steps;
+    j.save_every = save;
+    if (h->amp != 0.0) j.pulse = cmd::Pulse{h->t1, h->t2, h->amp, h->amp};
+    std::vector<GJob> jobs{j};
+    std::vector<long long> stats;
+    if (int rc = run_global(h, jobs, mode_of(method), h->abs_tol, h->rel_tol, h->max_steps, stats)) return rc;
+    if (rows_needed) *rows_needed = stats[0];
+    if (stats[3] != 0) return fail(CMD_ERR_NONFINITE, "step-size control failed (500 consecutive rejections)");
+    return CMD_OK;
+}
+
+bool resident_fits(const cmd_handle* h) { return pick_variant(h) >= 0; }
+
+}  // namespace
+
 int cmd_step(cmd_handle* h, double t, double dt, int method) {
     cmd::clear_error();
     if (int rc = check_handle(h, true)) return rc;
-    if (method != CMD_RK4) return fail(CMD_ERR_UNSUPPORTED, "cmd_step: only CMD_RK4 is implemented");
+    if (method != CMD_RK4 && method != CMD_DOPRI5_FIXED)
+        return fail(CMD_ERR_INVALID_ARG, "cmd_step takes a fixed-step method (CMD_RK4 or CMD_DOPRI5_FIXED)");
     if (!std::isfinite(t) || !std::isfinite(dt)) return fail(CMD_ERR_INVALID_ARG, "non-finite t or dt");
-    return run_single(h, t, dt, 1, 1, (double)h->N, false, false, true);
+    if (method == CMD_RK4 && resident_fits(h)) return run_single(h, t, dt, 1, 1, (double)h->N, false, false, true);
+    return run_global_single(h, method, t, t + dt, dt, 1, 1, 0, false, nullptr);
 }
 
 int cmd_integrate(cmd_handle* h, double T0, double T1, double dt, int64_t save_interval, int method,
                   double* times, double* obs, double* states, int64_t max_rows, int64_t* rows_out) {
     cmd::clear_error();
     if (int rc = check_handle(h, true)) return rc;
-    if (method != CMD_RK4) return fail(CMD_ERR_UNSUPPORTED, "cmd_integrate: only CMD_RK4 is implemented");
+    if (method != CMD_RK4 && method != CMD_DOPRI5_FIXED && method != CMD_RK45)
+        return fail(CMD_ERR_INVALID_ARG, "unknown integration method");
     if (save_interval <= 0 || !(dt > 0.0) || !std::isfinite(T0) || !std::isfinite(T1))
         return fail(CMD_ERR_INVALID_ARG, "bad integration window");
+    if (method == CMD_RK45) {
+        // rows = accepted steps + 1, known only afterwards
+        if (max_rows <= 0) {
+            if (rows_out) *rows_out = (h->max_steps > 0 ? h->max_steps : (int64_t)((T1 - T0) / dt) * 4 + 16) + 1;
+            return fail(CMD_ERR_INVALID_ARG, "max_rows too small");
+        }
+        int64_t needed = 0;
+        if (int rc = run_global_single(h, method, T0, T1, dt, 0, 1, max_rows, states != nullptr, &needed)) return rc;
+        if (rows_out) *rows_out = needed;
+        if (needed > max_rows) return fail(CMD_ERR_INVALID_ARG, "max_rows too small");
+        std::vector<double> rows((size_t)needed * 11);
+        CUDA_TRY(cudaMemcpy(rows.data(), h->grows.p, rows.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int64_t r = 0; r < needed; ++r) {
+            if (times) times[r] = rows[11 * r];
+            if (obs) std::memcpy(obs + 10 * r, &rows[11 * r + 1], 10 * sizeof(double));
+        }
+        if (states)
+            CUDA_TRY(cudaMemcpy(states, h->traj.p, needed * h->N * 3 * sizeof(double), cudaMemcpyDeviceToHost));
+        return CMD_OK;
+    }
     std::vector<double> grid;
     const int64_t n = count_steps(T0, T1, dt, 0.0, &grid);
     const int64_t rows = rows_for(n, save_interval);
     if (rows_out) *rows_out = rows;
     if (max_rows < rows) return fail(CMD_ERR_INVALID_ARG, "max_rows too small");
-    if (int rc = run_single(h, T0, dt, n, save_interval, (double)h->N, obs != nullptr, states != nullptr, true))
-        return rc;
+    if (method == CMD_RK4 && resident_fits(h)) {
+        if (int rc = run_single(h, T0, dt, n, save_interval, (double)h->N, obs != nullptr, states != nullptr, true))
+            return rc;
+        if (obs) CUDA_TRY(cudaMemcpy(obs, h->obs.p, rows * 10 * sizeof(double), cudaMemcpyDeviceToHost));
+    } else {
+        if (int rc = run_global_single(h, method, T0, T1, dt, n, save_interval, rows, states != nullptr, nullptr))
+            return rc;
+        if (obs) {
+            std::vector<double> r11((size_t)rows * 11);
+            CUDA_TRY(cudaMemcpy(r11.data(), h->grows.p, r11.size() * sizeof(double), cudaMemcpyDeviceToHost));
+            for (int64_t r = 0; r < rows; ++r) std::memcpy(obs + 10 * r, &r11[11 * r + 1], 10 * sizeof(double));
+        }
+    }
     if (times) {
         int64_t r = 0;
         for (int64_t k = 0; k < n; k += save_interval) times[r++] = grid[k];
         times[r] = grid[n];
     }
-    if (obs) CUDA_TRY(cudaMemcpy(obs, h->obs.p, rows * 10 * sizeof(double), cudaMemcpyDeviceToHost));
     if (states)
         CUDA_TRY(cudaMemcpy(states, h->traj.p, rows * h->N * 3 * sizeof(double), cudaMemcpyDeviceToHost));
+    return CMD_OK;
+}
+
+int cmd_run_uneven(cmd_traj_spec* specs, int64_t B, int method, double abs_tol, double rel_tol,
+                   int64_t max_steps) {
+    cmd::clear_error();
+    if (!specs || B <= 0) return fail(CMD_ERR_INVALID_ARG, "empty batch");
+    if (method != CMD_RK4 && method != CMD_DOPRI5_FIXED && method != CMD_RK45)
+        return fail(CMD_ERR_INVALID_ARG, "unknown integration method");
+    if (method == CMD_RK45 && (!(abs_tol >= 0.0) || !(rel_tol >= 0.0) || (abs_tol == 0.0 && rel_tol == 0.0)))
+        return fail(CMD_ERR_INVALID_ARG, "bad tolerances");
+    cmd_handle* owner = specs[0].lattice;
+    size_t in_total = 0, row_total = 0;
+    std::vector<size_t> ioff(B), roff(B);
+    std::vector<int64_t> nsteps(B, 0);
+    for (int64_t b = 0; b < B; ++b) {
+        cmd_traj_spec& sp = specs[b];
+        if (!sp.lattice || !sp.state || !sp.rows || sp.max_rows <= 0 || !(sp.dt > 0.0) || !(sp.T1 >= sp.T0))
+            return fail(CMD_ERR_INVALID_ARG, "bad trajectory spec");
+        for (int64_t i = 0; i < sp.lattice->N * 3; ++i)
+            if (!std::isfinite(sp.state[i])) return fail(CMD_ERR_NONFINITE, "non-finite initial spin");
+        ioff[b] = in_total;
+        in_total += (size_t)sp.lattice->N * 3;
+        roff[b] = row_total;
+        row_total += (size_t)sp.max_rows * 11;
+        if (method != CMD_RK45) nsteps[b] = count_steps(sp.T0, sp.T1, sp.dt, 0.0, nullptr);
+    }
+    if (int rc = owner->batch_states.ensure(2 * in_total * sizeof(double))) return rc;
+    if (int rc = owner->batch_out.ensure(row_total * sizeof(double))) return rc;
+    double* din = owner->batch_states.as<double>();
+    double* dout = din + in_total;
+    double* drows = owner->batch_out.as<double>();
+    std::vector<GJob> jobs(B);
+    for (int64_t b = 0; b < B; ++b) {
+        cmd_traj_spec& sp = specs[b];
+        CUDA_TRY(cudaMemcpyAsync(din + ioff[b], sp.state, sp.lattice->N * 3 * sizeof(double), cudaMemcpyHostToDevice,
+                                 owner->stream));
+        GJob& j = jobs[b];
+        j.h = sp.lattice;
+        j.y0 = din + ioff[b];
+        j.yout = dout + ioff[b];
+        j.rows = drows + roff[b];
+        j.max_rows = sp.max_rows;
+        j.T0 = sp.T0; j.T1 = sp.T1; j.dt0 = sp.dt;
+        j.n_steps = nsteps[b];
+        j.save_every = 1;
+        if (sp.a1 != 0.0 || sp.a2 != 0.0) j.pulse = cmd::Pulse{sp.t1, sp.t2, sp.a1, sp.a2};
+    }
+    std::vector<long long> stats;
+    if (int rc = run_global(owner, jobs, mode_of(method), abs_tol, rel_tol, max_steps, stats)) return rc;
+    bool overflow = false;
+    for (int64_t b = 0; b < B; ++b) {
+        cmd_traj_spec& sp = specs[b];
+        for (int q = 0; q < 4; ++q) sp.stats[q] = stats[4 * b + q];
+        const int64_t n = std::min<int64_t>(sp.stats[0], sp.max_rows);
+        overflow |= sp.stats[0] > sp.max_rows;
+        CUDA_TRY(cudaMemcpyAsync(sp.rows, drows + roff[b], n * 11 * sizeof(double), cudaMemcpyDeviceToHost, owner->stream));
+        if (sp.final_state)
+            CUDA_TRY(cudaMemcpyAsync(sp.final_state, dout + ioff[b], sp.lattice->N * 3 * sizeof(double),
+                                     cudaMemcpyDeviceToHost, owner->stream));
+    }
+    if (int rc = sync(owner)) return rc;
+    if (overflow) return fail(CMD_ERR_INVALID_ARG, "max_rows too small for some trajectory");
+    for (int64_t b = 0; b < B; ++b)
+        if (specs[b].stats[3] != 0) return fail(CMD_ERR_NONFINITE, "step-size control failed for some trajectory");
     return CMD_OK;
 }
 
@@ -779,8 +1124,13 @@ int run_batch_device(cmd_handle* h, const cmd_batch_desc* d, const cmd::Pulse* d
     r.pulses = d_pulses;
     r.width = d->width;
     r.freq = d->freq;
-    r.d1 = d->d1;
-    r.d2 = d->d2;
+    std::vector<double> d1c, d2c;
+    if (d->d1)
+        if (int rc = reduce_per_class(h, d->d1, 3, d1c, "pulse directions")) return rc;
+    if (d->d2)
+        if (int rc = reduce_per_class(h, d->d2, 3, d2c, "pulse directions")) return rc;
+    r.d1 = d->d1 ? d1c.data() : nullptr;
+    r.d2 = d->d2 ? d2c.data() : nullptr;
     r.n_sites = (double)h->N;
     return run_resident(h, r, st, launches);
 }
@@ -975,7 +1325,12 @@ int cmd_integrate_batched(cmd_handle* h, const double* init, const double* tau2,
     if (max_rows < rows) return fail(CMD_ERR_INVALID_ARG, "max_rows too small");
     std::vector<double> t1(B, h->t1), a(B, h->amp), obs((size_t)B * rows * 10);
     // Frames / AFM signs of the call override the lattice's for the observables.
-    if (int rc = upload_frames(h, frames ? frames : h->frames.data(), afm_signs ? afm_signs : h->afm.data()))
+    std::vector<double> frc, afc;
+    if (frames)
+        if (int rc = reduce_per_class(h, frames, 9, frc, "sublattice frames")) return rc;
+    if (afm_signs)
+        if (int rc = reduce_per_class(h, afm_signs, 1, afc, "AFM signs")) return rc;
+    if (int rc = upload_frames(h, frames ? frc.data() : h->frames.data(), afm_signs ? afc.data() : h->afm.data()))
         return rc;
     cmd_batch_desc d{};
     d.B = B;
@@ -983,7 +1338,15 @@ int cmd_integrate_batched(cmd_handle* h, const double* init, const double* tau2,
     d.shared_initial = 1;
     d.method = CMD_RK4;
     d.t1 = t1.data(); d.t2 = tau2; d.a1 = a.data(); d.a2 = a.data();
-    d.d1 = h->fd.data(); d.d2 = h->fd.data() + 3 * h->NA;
+    // h->fd is per class; expand to the caller's atoms for cmd_run_batch
+    const int ca = caller_atoms(h);
+    std::vector<double> e1(3 * (size_t)ca), e2(3 * (size_t)ca);
+    for (int at = 0; at < ca; ++at)
+        for (int c = 0; c < 3; ++c) {
+            e1[3 * at + c] = h->fd[3 * (at % h->NA) + c];
+            e2[3 * at + c] = h->fd[3 * h->NA + 3 * (at % h->NA) + c];
+        }
+    d.d1 = e1.data(); d.d2 = e2.data();
     d.width = h->width; d.freq = h->freq;
     d.T0 = T0; d.dt = dt;
     d.n_steps = n; d.save_interval = save_interval;

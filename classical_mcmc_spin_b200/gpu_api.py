@@ -146,25 +146,35 @@ def set_tolerances(handle, abs_tol, rel_tol, max_steps=0):
           "set_tolerances")
 
 
-def integrate_gpu(handle, T_start, T_end, dt, save_interval, method="rk4", with_states=True):
+def integrate_gpu(handle, T_start, T_end, dt, save_interval, method="rk4", with_states=True, max_rows=None):
     """integrate_gpu (lattice_gpu_api.h:117-125).
 
-    Returns ``(trajectory, obs)``: ``trajectory`` is the reference's list of
-    ``(t, state)`` pairs (empty when ``with_states`` is False) and ``obs`` the
+    Returns ``(trajectory, obs, times)``: ``trajectory`` is the reference's list
+    of ``(t, state)`` pairs (empty when ``with_states`` is False), ``obs`` the
     per-row observables {M_af, M_local, M_global, E/N} computed on the device.
+    Methods: "rk4", "dopri5" (the reference GPU's fixed-step Dormand-Prince)
+    and "rk45" (controlled Dormand-Prince with the CPU path's step control;
+    ``dt`` is the initial step, one row per accepted step).
     """
     rows = C.c_int64()
     m = _method(method)
-    rc = nat.lib().cmd_integrate(handle.ptr, float(T_start), float(T_end), float(dt), int(save_interval), m,
-                                 None, None, None, 0, C.byref(rows))
-    if rc not in (nat.CMD_OK, nat.CMD_ERR_INVALID_ARG) or rows.value <= 0:
-        check(rc, "integrate_gpu")
-    n = rows.value
+    L = nat.lib()
+    n = int(max_rows) if max_rows else 0
+    if n <= 0:
+        rc = L.cmd_integrate(handle.ptr, float(T_start), float(T_end), float(dt), int(save_interval), m,
+                             None, None, None, 0, C.byref(rows))
+        if rc not in (nat.CMD_OK, nat.CMD_ERR_INVALID_ARG) or rows.value <= 0:
+            check(rc, "integrate_gpu")
+        n = rows.value
     times = np.zeros(n)
     obs = np.zeros((n, 10))
     states = np.zeros((n, 3 * handle.N)) if with_states else None
-    check(nat.lib().cmd_integrate(handle.ptr, float(T_start), float(T_end), float(dt), int(save_interval), m,
-                                  dptr(times), dptr(obs), dptr(states), n, C.byref(rows)), "integrate_gpu")
+    # A controlled run that needs more than max_rows rows has advanced the state
+    # already; the error carries the row count it needed.
+    check(L.cmd_integrate(handle.ptr, float(T_start), float(T_end), float(dt), int(save_interval), m,
+                          dptr(times), dptr(obs), dptr(states), n, C.byref(rows)), "integrate_gpu")
+    n = rows.value
+    times, obs = times[:n], obs[:n]
     traj = [(float(times[r]), states[r]) for r in range(n)] if with_states else []
     return traj, obs, times
 
@@ -264,3 +274,37 @@ def run_batch(handle, states, n_steps, dt, T0=0.0, save_interval=1, t1=None, t2=
     d.final_states = fin.ctypes.data if fin is not None else None
     check(nat.lib().cmd_run_batch(handle.ptr, C.byref(d)), "cmd_run_batch")
     return obs, fin
+
+
+def run_uneven(specs, method="rk45", abs_tol=1e-10, rel_tol=1e-10, max_steps=0):
+    """Uneven batch (cmd_run_uneven): one persistent launch over trajectories on
+    different lattices.  ``specs``: list of dicts with keys handle, state, T0, T1,
+    dt and optional t1, t2, a1, a2, max_rows, want_final.  Returns a list of
+    (rows[n][11] = {t, M_af, M_local, M_global, E/N}, final_state or None, stats)."""
+    B = len(specs)
+    arr = (nat.TrajSpec * B)()
+    keep = []
+    for b, sp in enumerate(specs):
+        h = sp["handle"]
+        st = f64(sp["state"], 3 * h.N)
+        mr = int(sp.get("max_rows", (max_steps + 2) if max_steps else int((sp["T1"] - sp["T0"]) / sp["dt"]) + 2))
+        rows = np.zeros((mr, 11))
+        fin = np.zeros(3 * h.N) if sp.get("want_final", True) else None
+        keep.append((st, rows, fin))
+        a = arr[b]
+        a.lattice = h.ptr.value
+        a.state = st.ctypes.data
+        a.T0, a.T1, a.dt = float(sp["T0"]), float(sp["T1"]), float(sp["dt"])
+        a.t1, a.t2 = float(sp.get("t1", 0.0)), float(sp.get("t2", 0.0))
+        a.a1, a.a2 = float(sp.get("a1", 0.0)), float(sp.get("a2", 0.0))
+        a.rows = rows.ctypes.data
+        a.max_rows = mr
+        a.final_state = fin.ctypes.data if fin is not None else None
+    check(nat.lib().cmd_run_uneven(C.cast(arr, C.c_void_p), B, _method(method), float(abs_tol), float(rel_tol),
+                                   int(max_steps)), "cmd_run_uneven")
+    out = []
+    for b in range(B):
+        st, rows, fin = keep[b]
+        stats = tuple(int(x) for x in arr[b].stats)
+        out.append((rows[:stats[0]], fin, stats))
+    return out

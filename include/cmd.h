@@ -187,6 +187,32 @@ int cmd_run_batch_device(cmd_handle* h, const cmd_batch_desc* d, void* stream, i
 int cmd_layout_info(cmd_handle* h, int64_t* info);
 
 /*
+ * Uneven batch (no reference counterpart): trajectories on different lattices
+ * (different sizes, and up to two unit-cell types, e.g. Kitaev honeycomb and
+ * non-Kramers pyrochlore) in ONE persistent launch that pulls trajectories
+ * from a work queue, longest first.  Lattices of one unit-cell type must share
+ * their couplings, pulse directions, width and frequency (cmd_set_pulse).
+ * method: CMD_RK45 (controlled, T0..T1 from dt, tolerances below, at most
+ * max_steps accepted steps when > 0; a row after every accepted step) or
+ * CMD_RK4 / CMD_DOPRI5_FIXED (fixed dt, reference loop, a row every step).
+ * Host pointers.  stats: rows produced (may exceed max_rows: then only
+ * max_rows are written and the call returns CMD_ERR_INVALID_ARG), accepted
+ * steps, rejected steps, status (0 ok, 1 step-size control failed).
+ */
+typedef struct cmd_traj_spec {
+    cmd_handle* lattice;
+    const double* state;         /* [N*3] initial spins                          */
+    double T0, T1, dt;
+    double t1, t2, a1, a2;       /* pulse pair; a1 = a2 = 0: no drive            */
+    double* rows;                /* [max_rows][11] = {t, M_af, M_local, M_global, E/N} */
+    int64_t max_rows;
+    double* final_state;         /* [N*3] or NULL                                */
+    int64_t stats[4];
+} cmd_traj_spec;
+int cmd_run_uneven(cmd_traj_spec* specs, int64_t B, int method, double abs_tol, double rel_tol,
+                   int64_t max_steps);
+
+/*
  * Autotuner over the resident-kernel variants compiled into the library
  * (cells per thread x threads per CTA x CTAs per SM x own stage input kept in
  * registers or re-read from shared memory).  No reference counterpart.

@@ -231,10 +231,10 @@ def test_errors_are_status_codes(api, native):
     api.set_gpu_spins(h, _spins(lat.lattice_size, 1))
     with pytest.raises(ValueError):
         api.step_gpu(h, 0.0, 0.01, "ssprk53")
-    big = Lattice.kitaev(48, 48, 1).to_gpu()
-    api.set_gpu_spins(big, _spins(4608, 1))
+    odd = Lattice.kitaev(4, 4, 1, J2_A=0.1, J2_B=0.1).to_gpu()    # 9 bonds/site: no kernel instance
+    api.set_gpu_spins(odd, _spins(32, 1))
     with pytest.raises(CmdError) as e:
-        api.step_gpu(big, 0.0, 0.01)
+        api.step_gpu(odd, 0.0, 0.01)
     assert e.value.code == native.CMD_ERR_UNSUPPORTED
 
 
@@ -274,3 +274,23 @@ def test_autotune_picks_a_fitting_variant(api, oracle):
     assert best in fits and ms[best] > 0
     assert all((ms[i] > 0) == (i in fits) for i in range(len(ms)))
     assert h.get_variant() == best
+
+
+def test_cubic_pyrochlore_cell_matches_oracle(api, oracle):
+    """16-site conventional cubic cells, grouped into the 4-site kernel classes."""
+    kw = dict(h=0.2, field_direction=R111, Jzz=1.0, Jpm=0.05, Jpmpm=0.02, cubic=True)
+    lat, o = _pair(oracle, "pyro", (2, 2, 2), **kw)
+    s0 = _spins(lat.lattice_size, 22)
+    fin16 = np.tile(R111, 16)
+    fd = lat.rotate_pulse(fin16, fin16)
+    h = lat.to_gpu()
+    assert h.layout_info()["sites_per_group"] == 4
+    api.set_gpu_spins(h, s0)
+    api.set_gpu_pulse(h, fd, 0.4, 0.5, 0.0, 0.2, 0.7)
+    _, obs, times = api.integrate_gpu(h, 0.0, 1.4975, 0.005, 5, "rk4", with_states=False)
+    o.set_pulse(fin16, 0.2, fin16, 0.7, 0.4, 0.5, 0.0)
+    rows, fin = o.md_rk4(s0, 0.0, 1.4975, 0.005, 5, gpu_loop=True)
+    assert len(rows) == len(obs)
+    assert np.abs(obs[:, :9] - rows[:, 1:10]).max() <= TOL_M
+    assert np.abs(obs[:, 9] - rows[:, 10]).max() <= TOL_M
+    assert np.abs(api.get_gpu_spins(h) - fin).max() <= TOL_S

@@ -146,3 +146,14 @@ def test_rotate_pulse_is_frame_times_field(native):
     R = lat.sublattice_frames
     np.testing.assert_allclose(fd[:3], R[0] @ R111, atol=1e-15)
     np.testing.assert_allclose(fd[6:9], R[0] @ (2 * R111), atol=1e-15)
+
+
+def test_layout_plan_groups_the_cubic_pyrochlore_cell(native):
+    """The 16-site cubic cell is 4 FCC translations of the 4-site group: it maps onto
+    the 4-atom kernels (same couplings, fields and frames per sublattice class)."""
+    lat = Lattice.pyrochlore_non_kramer(2, 2, 2, cubic=True, h=0.2, field_direction=R111, Jzz=1.0, Jpm=0.05,
+                                        Jpmpm=0.02)
+    assert lat.N_atoms == 16
+    rc, info, msg = _plan(lat)
+    assert rc == nat.CMD_OK, msg
+    assert list(info[[0, 1, 2, 6]]) == [4, lat.lattice_size // 4, 6, 3]
