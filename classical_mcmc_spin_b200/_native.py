@@ -84,6 +84,7 @@ _SIGS = {
     "cmd_layout_info": (C.c_int, [C.c_void_p, _I64]),
     "cmd_plan_layout": (C.c_int, [C.POINTER(LatticeDesc), _I64]),
     "cmd_run_uneven": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.c_double, C.c_double, C.c_int64]),
+    "cmd_adjoint_rk4": (C.c_int, [C.c_void_p, C.c_void_p]),
     "cmd_variant_count": (C.c_int, []),
     "cmd_variant_info": (C.c_int, [C.c_void_p, C.c_int32, C.c_char_p, C.c_int32, _I32]),
     "cmd_set_variant": (C.c_int, [C.c_void_p, C.c_int32]),

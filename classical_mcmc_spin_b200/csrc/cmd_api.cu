@@ -13,6 +13,7 @@
 #include "cmd_internal.h"
 #include "rk4_resident.cuh"
 #include "rk_global.cuh"
+#include "rk_adjoint.cuh"
 
 #include <cuda_runtime.h>
 
@@ -58,6 +59,7 @@ struct Layout {
     std::vector<int> zc;        // slots per atom
     std::vector<double> J;      // [NA][Z][9]
     std::vector<int> nbr;       // [G][NA][Z-LZ] shared-memory offsets
+    std::vector<int> slot_entry;  // [NA][Z] ELL entry at cell 0 each slot came from
     bool uniform = false;
     std::string why;            // reason when not uniform
 };
@@ -100,6 +102,7 @@ struct cmd_handle {
     DevBuf state, nbr, obs, traj, batch_states, batch_out, pulses, scratch;
     DevBuf dframes, dafm, times, drive, raw, tune_states, tune_obs;
     DevBuf gwork, gmeta, gstat, grows, gqueue;
+    DevBuf awork, ackpt, aseg, amloc, aout, ameta, ain;
     bool has_state = false;
     int variant = -1;           // resident-kernel variant; -1 = heuristic default
     // pulse (set_gpu_pulse)
@@ -153,14 +156,14 @@ void analyse_as(const cmd_lattice_desc& d, int NA, Layout& L) {
         }
     }
     // canonical (cell 0) slot lists per atom
-    struct Slot { const double* J; int b; int64_t p0; };   // p0: partner seen from cell 0
+    struct Slot { const double* J; int b; int64_t p0; int e; };   // p0: partner seen from cell 0; e: ELL entry
     std::vector<std::vector<Slot>> canon(NA);
     for (int a = 0; a < NA; ++a) {
         for (int64_t n = 0; n < d.counts[a]; ++n) {
             const double* J = &d.bilinear[9 * (a * (int64_t)zmax + n)];
             if (mat_zero(J)) continue;
             const int64_t p = d.partners[a * (int64_t)zmax + n];
-            canon[a].push_back(Slot{J, (int)(p % NA), p});
+            canon[a].push_back(Slot{J, (int)(p % NA), p, (int)n});
         }
     }
     // Try local-first ordering: slot n < NA-1 of atom a bonds to atom (a+1+n)%NA
@@ -241,8 +244,10 @@ void analyse_as(const cmd_lattice_desc& d, int NA, Layout& L) {
         L.Z = Z;
         L.zc.resize(NA);
         L.J.assign((size_t)NA * std::max(Z, 1) * 9, 0.0);
+        L.slot_entry.assign((size_t)NA * std::max(Z, 1), -1);
         for (int a = 0; a < NA; ++a) {
             L.zc[a] = (int)order[a].size();
+            for (int s2 = 0; s2 < (int)order[a].size(); ++s2) L.slot_entry[(size_t)a * Z + s2] = order[a][s2].e;
             for (int s = 0; s < (int)order[a].size(); ++s)
                 std::memcpy(&L.J[((size_t)a * Z + s) * 9], order[a][s].J, 9 * sizeof(double));
         }
@@ -778,7 +783,8 @@ int cmd_destroy(cmd_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (DevBuf* b : {&h->state, &h->nbr, &h->obs, &h->traj, &h->batch_states, &h->batch_out,
                       &h->pulses, &h->scratch, &h->dframes, &h->dafm, &h->times, &h->drive, &h->raw,
-                      &h->tune_states, &h->tune_obs, &h->gwork, &h->gmeta, &h->gstat, &h->grows, &h->gqueue})
+                      &h->tune_states, &h->tune_obs, &h->gwork, &h->gmeta, &h->gstat, &h->grows, &h->gqueue,
+                      &h->awork, &h->ackpt, &h->aseg, &h->amloc, &h->aout, &h->ameta, &h->ain})
         b->release();
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -1185,6 +1191,139 @@ int cmd_run_batch_device(cmd_handle* h, const cmd_batch_desc* d, void* stream, i
     if ((d->d1 || d->d2) && h->NA > 64) return fail(CMD_ERR_UNSUPPORTED, "drive directions limited to 64 atoms");
     const cmd::Pulse* d_pulses = (d->d1 || d->d2) ? reinterpret_cast<const cmd::Pulse*>(d->pulse4) : nullptr;
     return run_batch_device(h, d, d_pulses, st, launches);
+}
+
+
+}  // extern "C"
+
+namespace {
+
+constexpr int kAdjParams = 5;
+
+template <int NAT, int Z, int LZ>
+int launch_adjoint(cmd_handle* h, const cmd::AdjArgs& a, const std::vector<double>& DJ, const std::vector<double>& DB,
+                   const std::vector<double>& DA, bool has_DA, int64_t B) {
+    cmd::Couplings<NAT, Z> cp;
+    fill_couplings<NAT, Z>(h, h->fd.data(), h->fd.data() + 3 * h->NA, cp);
+    cmd::adjoint_forward_kernel<NAT, Z, LZ><<<(unsigned)B, 256, 0, h->stream>>>(cp, a);
+    CUDA_TRY(cudaGetLastError());
+    if (a.forward_only) return CMD_OK;
+    cmd::ParamDerivs<NAT, Z, kAdjParams> pd;
+    std::memset(&pd, 0, sizeof(pd));
+    for (int q = 0; q < kAdjParams; ++q)
+        for (int at = 0; at < NAT; ++at) {
+            for (int s = 0; s < Z; ++s)
+                std::memcpy(pd.DJ[q][at][s], &DJ[(((size_t)q * NAT + at) * Z + s) * 9], 9 * sizeof(double));
+            std::memcpy(pd.DB[q][at], &DB[((size_t)q * NAT + at) * 3], 3 * sizeof(double));
+            std::memcpy(pd.DA[q][at], &DA[((size_t)q * NAT + at) * 9], 9 * sizeof(double));
+        }
+    pd.has_DA = has_DA;
+    cmd::adjoint_backward_kernel<NAT, Z, LZ, kAdjParams><<<(unsigned)B, 256, 0, h->stream>>>(cp, pd, a);
+    CUDA_TRY(cudaGetLastError());
+    return CMD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cmd_adjoint_rk4(cmd_handle* h, const cmd_adjoint_desc* d) {
+    cmd::clear_error();
+    if (int rc = check_handle(h, false)) return rc;
+    if (!d || d->B <= 0 || !d->states || !d->target || !d->loss || d->n_steps <= 0 || !(d->dt > 0.0))
+        return fail(CMD_ERR_INVALID_ARG, "bad adjoint description");
+    if (d->n_params < 0 || d->n_params > kAdjParams || (d->n_params > 0 && (!d->dparams || !d->grad)))
+        return fail(CMD_ERR_INVALID_ARG, "n_params must be 0..5 with derivative lattices and a grad buffer");
+    const int ty = global_type(h->lay);
+    if (ty < 0) return no_instance(h->lay);
+    const int NA = h->NA, Z = h->lay.Z;
+    // derivative tables per (parameter, atom class, slot) from the theta = e_q lattices
+    std::vector<double> DJ((size_t)kAdjParams * NA * Z * 9, 0.0), DB((size_t)kAdjParams * NA * 3, 0.0),
+        DA((size_t)kAdjParams * NA * 9, 0.0);
+    bool has_DA = false;
+    for (int q = 0; q < d->n_params; ++q) {
+        const cmd_lattice_desc& p = d->dparams[q];
+        if (p.lattice_size != h->N || !p.counts || !p.partners || !p.bilinear || !p.field || !p.onsite)
+            return fail(CMD_ERR_INVALID_ARG, "derivative lattice does not match the handle's lattice");
+        for (int a = 0; a < NA; ++a) {
+            for (int s = 0; s < h->lay.zc[a]; ++s) {
+                const int e = h->lay.slot_entry[(size_t)a * Z + s];
+                if (e < 0 || e >= p.counts[a]) return fail(CMD_ERR_INVALID_ARG, "derivative lattice bond tables differ");
+                std::memcpy(&DJ[(((size_t)q * NA + a) * Z + s) * 9], &p.bilinear[((int64_t)a * p.max_bilinear + e) * 9],
+                            9 * sizeof(double));
+            }
+            std::memcpy(&DB[((size_t)q * NA + a) * 3], &p.field[3 * a], 3 * sizeof(double));
+            std::memcpy(&DA[((size_t)q * NA + a) * 9], &p.onsite[9 * a], 9 * sizeof(double));
+            for (int k = 0; k < 9; ++k) has_DA |= p.onsite[9 * a + k] != 0.0;
+        }
+    }
+    const int64_t B = d->B, S = d->n_steps, N3 = h->N * 3, V = N3;
+    int64_t C = d->checkpoint_every > 0 ? d->checkpoint_every : (int64_t)std::ceil(std::sqrt((double)S));
+    C = std::max<int64_t>(1, std::min(C, S));
+    const int64_t K = (S + C - 1) / C;
+    const bool fwd_only = d->forward_only != 0;
+    if (int rc = h->awork.ensure((size_t)B * 13 * V * sizeof(double))) return rc;
+    if (!fwd_only) {
+        if (int rc = h->ackpt.ensure((size_t)B * K * V * sizeof(double))) return rc;
+        if (int rc = h->aseg.ensure((size_t)B * C * V * sizeof(double))) return rc;
+    }
+    if (int rc = h->amloc.ensure((size_t)B * (S + 1) * 3 * sizeof(double))) return rc;
+    if (int rc = h->aout.ensure((size_t)B * (1 + kAdjParams) * sizeof(double))) return rc;
+    if (int rc = h->ain.ensure(((size_t)B * N3 + (size_t)B * (S + 1) * 3 + (S + 1)) * sizeof(double))) return rc;
+    if (int rc = h->ameta.ensure((size_t)B * sizeof(cmd::AdjTraj))) return rc;
+    for (int64_t i = 0; i < B * N3; ++i)
+        if (!std::isfinite(d->states[i])) return fail(CMD_ERR_NONFINITE, "non-finite initial spin");
+    double* din = h->ain.as<double>();
+    double* dtgt = din + B * N3;
+    double* dtimes = dtgt + B * (S + 1) * 3;
+    std::vector<double> times((size_t)S + 1);
+    double t = d->T0;
+    for (int64_t n = 0; n <= S; ++n) { times[n] = t; t += d->dt; }
+    CUDA_TRY(cudaMemcpyAsync(din, d->states, B * N3 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(dtgt, d->target, B * (S + 1) * 3 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(dtimes, times.data(), times.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    std::vector<cmd::AdjTraj> tr(B);
+    double* dout = h->aout.as<double>();
+    for (int64_t b = 0; b < B; ++b) {
+        cmd::AdjTraj& T = tr[b];
+        T.y0 = din + b * N3;
+        T.target = dtgt + b * (S + 1) * 3;
+        T.ckpt = fwd_only ? nullptr : h->ackpt.as<double>() + b * K * V;
+        T.seg = fwd_only ? nullptr : h->aseg.as<double>() + b * C * V;
+        T.work = h->awork.as<double>() + b * 13 * V;
+        T.mloc = h->amloc.as<double>() + b * (S + 1) * 3;
+        T.loss = dout + b * (1 + kAdjParams);
+        T.grad = dout + b * (1 + kAdjParams) + 1;
+    }
+    CUDA_TRY(cudaMemcpyAsync(h->ameta.p, tr.data(), B * sizeof(cmd::AdjTraj), cudaMemcpyHostToDevice, h->stream));
+    cmd::AdjArgs a{};
+    a.traj = h->ameta.as<cmd::AdjTraj>();
+    a.B = (int)B;
+    a.G = (int)h->lay.G;
+    a.nbr = h->nbr.as<int>();
+    a.times = dtimes;
+    a.n_steps = S;
+    a.ckpt_every = C;
+    a.dt = d->dt;
+    if (h->amp != 0.0) a.pulse = cmd::Pulse{h->t1, h->t2, h->amp, h->amp};
+    a.width = h->width;
+    a.freq = h->freq;
+    a.forward_only = fwd_only;
+    int rc = ty == 0 ? launch_adjoint<2, 3, 1>(h, a, DJ, DB, DA, has_DA, B)
+                     : launch_adjoint<4, 6, 3>(h, a, DJ, DB, DA, has_DA, B);
+    if (rc != CMD_OK) return rc;
+    std::vector<double> out((size_t)B * (1 + kAdjParams));
+    CUDA_TRY(cudaMemcpyAsync(out.data(), dout, out.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (d->m_local)
+        CUDA_TRY(cudaMemcpyAsync(d->m_local, h->amloc.p, B * (S + 1) * 3 * sizeof(double), cudaMemcpyDeviceToHost,
+                                 h->stream));
+    if (int rc2 = sync(h)) return rc2;
+    for (int64_t b = 0; b < B; ++b) {
+        d->loss[b] = out[b * (1 + kAdjParams)];
+        if (!fwd_only)
+            for (int q = 0; q < d->n_params; ++q) d->grad[b * d->n_params + q] = out[b * (1 + kAdjParams) + 1 + q];
+    }
+    return CMD_OK;
 }
 
 int cmd_plan_layout(const cmd_lattice_desc* d, int64_t* info) {

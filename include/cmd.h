@@ -213,6 +213,36 @@ int cmd_run_uneven(cmd_traj_spec* specs, int64_t B, int method, double abs_tol, 
                    int64_t max_steps);
 
 /*
+ * Discrete adjoint of the RK4 trajectory (no reference counterpart; the
+ * reference has no gradients).  For each of B initial states, RK4 (the
+ * reference GPU stepper's arithmetic, t += dt) for n_steps steps from T0 under
+ * h's couplings and pulse, and the loss
+ *     L_b = sum_{n=0..n_steps} |M_local(t_n) - target_b[n]|^2,
+ * with its gradient with respect to n_params (<= 5) coupling parameters.  The
+ * couplings must depend linearly on the parameters; parameter q is described
+ * by the lattice built with theta = e_q (same bond tables as h's lattice):
+ * its couplings are dJ/dtheta_q, its field dB/dtheta_q, its onsite terms
+ * dA/dtheta_q.  Checkpoints every checkpoint_every steps (0: ~sqrt(n_steps));
+ * the backward sweep recomputes each segment.  forward_only != 0 runs only the
+ * forward pass (loss, m_local; grad untouched).  Host pointers.
+ */
+typedef struct cmd_adjoint_desc {
+    int64_t B;
+    const double* states;              /* [B][N*3]                               */
+    double T0, dt;
+    int64_t n_steps;
+    const double* target;              /* [B][n_steps+1][3]                      */
+    int64_t checkpoint_every;
+    int32_t n_params;
+    int32_t forward_only;
+    const cmd_lattice_desc* dparams;   /* [n_params]                             */
+    double* loss;                      /* [B] out                                */
+    double* grad;                      /* [B][n_params] out                      */
+    double* m_local;                   /* [B][n_steps+1][3] out, or NULL          */
+} cmd_adjoint_desc;
+int cmd_adjoint_rk4(cmd_handle* h, const cmd_adjoint_desc* d);
+
+/*
  * Autotuner over the resident-kernel variants compiled into the library
  * (cells per thread x threads per CTA x CTAs per SM x own stage input kept in
  * registers or re-read from shared memory).  No reference counterpart.

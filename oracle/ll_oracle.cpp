@@ -872,3 +872,119 @@ void ora_batch_rk4(const ora_lattice* L, double* states, int B, const double* t1
 }
 
 }  // extern "C"
+
+// ---- tangent-linear reference gradient --------------------------------------
+namespace {
+
+// dY = d(f)(Y)[Ydot] + (df/dtheta_q)(Y) for one parameter; reference RHS form:
+// f_i = H_i x S_i, H_i = -B_i + 2 A_i S_i + sum_n J_n S_p(n) - drive(t).
+void rhs_tangent(const ora_lattice* L, const ora_lattice* D, const double* Y, const double* Yd, double t,
+                 double* out) {
+    const bool drive_active = (L->amp != 0.0);
+    double f1 = 0.0, f2 = 0.0;
+    if (drive_active) drive_factors(L, t, f1, f2);
+    for (size_t i = 0; i < L->N; ++i) {
+        double H[3], Hd[3];
+        local_field_site(L, Y, i, H);
+        if (drive_active) {
+            const size_t atom = i % L->n_atoms;
+            for (int d = 0; d < 3; ++d) H[d] -= L->fd[0][3 * atom + d] * f1 + L->fd[1][3 * atom + d] * f2;
+        }
+        // linearised field: couplings of L on Yd, plus derivative couplings of D on Y
+        for (int d = 0; d < 3; ++d) Hd[d] = -D->field[3 * i + d];
+        for (int d = 0; d < 3; ++d)
+            for (int d2 = 0; d2 < 3; ++d2)
+                Hd[d] += 2.0 * L->onsite[9 * i + 3 * d + d2] * Yd[3 * i + d2] +
+                         2.0 * D->onsite[9 * i + 3 * d + d2] * Y[3 * i + d2];
+        for (size_t k = L->off[i]; k < L->off[i + 1]; ++k) {
+            const double* J = &L->J[9 * k];
+            const double* DJ = &D->J[9 * k];
+            const double* P = Y + 3 * L->part[k];
+            const double* Pd = Yd + 3 * L->part[k];
+            for (int d = 0; d < 3; ++d)
+                for (int d2 = 0; d2 < 3; ++d2) Hd[d] += J[3 * d + d2] * Pd[d2] + DJ[3 * d + d2] * P[d2];
+        }
+        const double* S = Y + 3 * i;
+        const double* Sd = Yd + 3 * i;
+        out[3 * i + 0] = Hd[1] * S[2] - Hd[2] * S[1] + H[1] * Sd[2] - H[2] * Sd[1];
+        out[3 * i + 1] = Hd[2] * S[0] - Hd[0] * S[2] + H[2] * Sd[0] - H[0] * Sd[2];
+        out[3 * i + 2] = Hd[0] * S[1] - Hd[1] * S[0] + H[0] * Sd[1] - H[1] * Sd[0];
+    }
+}
+
+void mloc(const ora_lattice* L, const double* x, double* m) {
+    m[0] = m[1] = m[2] = 0.0;
+    for (size_t i = 0; i < L->N; ++i)
+        for (int d = 0; d < 3; ++d) m[d] += x[3 * i + d];
+    for (int d = 0; d < 3; ++d) m[d] /= double(L->N);
+}
+
+}  // namespace
+
+extern "C" double ora_loss(const ora_lattice* L, const double* state0, double T0, double dt, long nsteps,
+                           const double* target) {
+    const size_t n = 3 * L->N;
+    std::vector<double> y(state0, state0 + n);
+    Work w(n);
+    double loss = 0.0, m[3], t = T0;
+    for (long s = 0; s <= nsteps; ++s) {
+        mloc(L, y.data(), m);
+        for (int d = 0; d < 3; ++d) loss += (m[d] - target[3 * s + d]) * (m[d] - target[3 * s + d]);
+        if (s == nsteps) break;
+        rk4_step_gpu_form(L, y.data(), t, dt, w);
+        t += dt;
+    }
+    return loss;
+}
+
+extern "C" double ora_loss_grad_tlm(const ora_lattice* L, const ora_lattice* const* D, int nq,
+                                    const double* state0, double T0, double dt, long nsteps,
+                                    const double* target, double* grad) {
+    const size_t n = 3 * L->N;
+    std::vector<double> y(state0, state0 + n), tmp(n), k1(n), k2(n), k3(n), k4(n);
+    std::vector<std::vector<double>> yd(nq, std::vector<double>(n, 0.0));
+    std::vector<double> Yd(n), kd1(n), kd2(n), kd3(n), kd4(n);
+    for (int q = 0; q < nq; ++q) grad[q] = 0.0;
+    double loss = 0.0, m[3], t = T0;
+    const double invN = 1.0 / double(L->N);
+    for (long s = 0; s <= nsteps; ++s) {
+        mloc(L, y.data(), m);
+        double r[3];
+        for (int d = 0; d < 3; ++d) {
+            r[d] = m[d] - target[3 * s + d];
+            loss += r[d] * r[d];
+        }
+        for (int q = 0; q < nq; ++q) {           // dL/dtheta += 2 r . dM/dtheta
+            double dm[3] = {0, 0, 0};
+            for (size_t i = 0; i < L->N; ++i)
+                for (int d = 0; d < 3; ++d) dm[d] += yd[q][3 * i + d];
+            for (int d = 0; d < 3; ++d) grad[q] += 2.0 * r[d] * dm[d] * invN;
+        }
+        if (s == nsteps) break;
+        // stages of the GPU-form RK4 step (integrator.cuh:115-139) and their tangents
+        rhs(L, y.data(), k1.data(), t);
+        std::vector<double> Y2(n), Y3(n), Y4(n);
+        for (size_t i = 0; i < n; ++i) Y2[i] = 1.0 * y[i] + (0.5 * dt) * k1[i];
+        rhs(L, Y2.data(), k2.data(), t + 0.5 * dt);
+        for (size_t i = 0; i < n; ++i) Y3[i] = 1.0 * y[i] + (0.5 * dt) * k2[i];
+        rhs(L, Y3.data(), k3.data(), t + 0.5 * dt);
+        for (size_t i = 0; i < n; ++i) Y4[i] = 1.0 * y[i] + dt * k3[i];
+        rhs(L, Y4.data(), k4.data(), t + dt);
+        for (int q = 0; q < nq; ++q) {
+            std::vector<double>& v = yd[q];
+            rhs_tangent(L, D[q], y.data(), v.data(), t, kd1.data());
+            for (size_t i = 0; i < n; ++i) Yd[i] = v[i] + (0.5 * dt) * kd1[i];
+            rhs_tangent(L, D[q], Y2.data(), Yd.data(), t + 0.5 * dt, kd2.data());
+            for (size_t i = 0; i < n; ++i) Yd[i] = v[i] + (0.5 * dt) * kd2[i];
+            rhs_tangent(L, D[q], Y3.data(), Yd.data(), t + 0.5 * dt, kd3.data());
+            for (size_t i = 0; i < n; ++i) Yd[i] = v[i] + dt * kd3[i];
+            rhs_tangent(L, D[q], Y4.data(), Yd.data(), t + dt, kd4.data());
+            const double c = dt / 6.0;
+            for (size_t i = 0; i < n; ++i) v[i] += c * (kd1[i] + 2.0 * kd2[i] + 2.0 * kd3[i] + kd4[i]);
+        }
+        const double c = dt / 6.0;
+        for (size_t i = 0; i < n; ++i) y[i] += c * (k1[i] + 2.0 * k2[i] + 2.0 * k3[i] + k4[i]);
+        t += dt;
+    }
+    return loss;
+}

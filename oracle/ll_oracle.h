@@ -160,6 +160,19 @@ void ora_batch_rk4(const ora_lattice* L, double* states, int B, const double* t1
                    double width, double freq, const double* dir1, const double* dir2,
                    double T0, double dt, long nsteps, double* obs, int with_energy);
 
+/* ---- gradient references for the discrete adjoint (tests only) ----
+ * Loss L = sum_{r=0..nsteps} |M_local(y_r) - target_r|^2 over the GPU-form RK4
+ * trajectory (t_r accumulated, t += dt) from state0 under L's couplings and
+ * drive.  dparam[q] are lattices with the same bond tables built at theta = e_q:
+ * their coupling entries are dJ/dtheta_q and their fields dB/dtheta_q.
+ * Forward-mode tangent linear model: grad[q] = dL/dtheta_q.  Returns L. */
+double ora_loss_grad_tlm(const ora_lattice* L, const ora_lattice* const* dparam, int nq,
+                         const double* state0, double T0, double dt, long nsteps,
+                         const double* target, double* grad);
+/* The loss alone (for finite differences). */
+double ora_loss(const ora_lattice* L, const double* state0, double T0, double dt, long nsteps,
+                const double* target);
+
 #ifdef __cplusplus
 }
 #endif

@@ -94,6 +94,9 @@ def lib() -> C.CDLL:
         "ora_pulse_drive": (C.c_long, [C.c_void_p, _D, _D, C.c_double, _D, C.c_double, C.c_int, C.c_double,
                                        C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
                                        C.c_int, C.c_double, C.c_double, _D, C.c_long]),
+        "ora_loss": (C.c_double, [C.c_void_p, _D, C.c_double, C.c_double, C.c_long, _D]),
+        "ora_loss_grad_tlm": (C.c_double, [C.c_void_p, C.POINTER(C.c_void_p), C.c_int, _D, C.c_double, C.c_double,
+                                           C.c_long, _D, _D]),
         "ora_batch_rk4": (None, [C.c_void_p, _D, C.c_int, _D, _D, _D, _D, C.c_double, C.c_double, C.c_double,
                                  _D, _D, C.c_double, C.c_double, C.c_long, _D, C.c_int]),
     }
@@ -277,6 +280,21 @@ class OracleLattice:
                               _p(_arr(dir1, 3 * self.n_atoms)), _p(_arr(dir2, 3 * self.n_atoms)), float(T0),
                               float(dt), int(nsteps), _p(obs) if obs is not None else None, int(with_energy))
         return st, obs
+
+
+def loss(L, state0, T0, dt, nsteps, target):
+    return float(lib().ora_loss(L.h, _p(_arr(state0, 3 * L.N)), float(T0), float(dt), int(nsteps),
+                                _p(_arr(target, 3 * (nsteps + 1)))))
+
+
+def loss_grad_tlm(L, dparams, state0, T0, dt, nsteps, target):
+    """(loss, dL/dtheta) by the tangent-linear model; dparams: OracleLattices built at theta = e_q."""
+    nq = len(dparams)
+    arr = (C.c_void_p * nq)(*[d.h for d in dparams])
+    g = np.zeros(nq)
+    val = lib().ora_loss_grad_tlm(L.h, arr, nq, _p(_arr(state0, 3 * L.N)), float(T0), float(dt), int(nsteps),
+                                  _p(_arr(target, 3 * (nsteps + 1))), _p(g))
+    return float(val), g
 
 
 def set_threads(n: int):
