@@ -1205,7 +1205,7 @@ int launch_adjoint(cmd_handle* h, const cmd::AdjArgs& a, const std::vector<doubl
                    const std::vector<double>& DA, bool has_DA, int64_t B) {
     cmd::Couplings<NAT, Z> cp;
     fill_couplings<NAT, Z>(h, h->fd.data(), h->fd.data() + 3 * h->NA, cp);
-    cmd::adjoint_forward_kernel<NAT, Z, LZ><<<(unsigned)B, 256, 0, h->stream>>>(cp, a);
+    cmd::adjoint_forward_kernel<NAT, Z, LZ><<<(unsigned)B, cmd::kAdjThreads, 0, h->stream>>>(cp, a);
     CUDA_TRY(cudaGetLastError());
     if (a.forward_only) return CMD_OK;
     cmd::ParamDerivs<NAT, Z, kAdjParams> pd;
@@ -1218,7 +1218,7 @@ int launch_adjoint(cmd_handle* h, const cmd::AdjArgs& a, const std::vector<doubl
             std::memcpy(pd.DA[q][at], &DA[((size_t)q * NAT + at) * 9], 9 * sizeof(double));
         }
     pd.has_DA = has_DA;
-    cmd::adjoint_backward_kernel<NAT, Z, LZ, kAdjParams><<<(unsigned)B, 256, 0, h->stream>>>(cp, pd, a);
+    cmd::adjoint_backward_kernel<NAT, Z, LZ, kAdjParams><<<(unsigned)B, cmd::kAdjThreads, 0, h->stream>>>(cp, pd, a);
     CUDA_TRY(cudaGetLastError());
     return CMD_OK;
 }
@@ -1262,10 +1262,10 @@ int cmd_adjoint_rk4(cmd_handle* h, const cmd_adjoint_desc* d) {
     C = std::max<int64_t>(1, std::min(C, S));
     const int64_t K = (S + C - 1) / C;
     const bool fwd_only = d->forward_only != 0;
-    if (int rc = h->awork.ensure((size_t)B * 13 * V * sizeof(double))) return rc;
+    if (int rc = h->awork.ensure((size_t)B * 5 * V * sizeof(double))) return rc;
     if (!fwd_only) {
         if (int rc = h->ackpt.ensure((size_t)B * K * V * sizeof(double))) return rc;
-        if (int rc = h->aseg.ensure((size_t)B * C * V * sizeof(double))) return rc;
+        if (int rc = h->aseg.ensure((size_t)B * C * 4 * V * sizeof(double))) return rc;
     }
     if (int rc = h->amloc.ensure((size_t)B * (S + 1) * 3 * sizeof(double))) return rc;
     if (int rc = h->aout.ensure((size_t)B * (1 + kAdjParams) * sizeof(double))) return rc;
@@ -1289,8 +1289,8 @@ int cmd_adjoint_rk4(cmd_handle* h, const cmd_adjoint_desc* d) {
         T.y0 = din + b * N3;
         T.target = dtgt + b * (S + 1) * 3;
         T.ckpt = fwd_only ? nullptr : h->ackpt.as<double>() + b * K * V;
-        T.seg = fwd_only ? nullptr : h->aseg.as<double>() + b * C * V;
-        T.work = h->awork.as<double>() + b * 13 * V;
+        T.seg = fwd_only ? nullptr : h->aseg.as<double>() + b * C * 4 * V;
+        T.work = h->awork.as<double>() + b * 5 * V;
         T.mloc = h->amloc.as<double>() + b * (S + 1) * 3;
         T.loss = dout + b * (1 + kAdjParams);
         T.grad = dout + b * (1 + kAdjParams) + 1;

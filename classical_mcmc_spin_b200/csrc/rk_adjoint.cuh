@@ -25,13 +25,24 @@
 // source and J^T at the partner, so sum_{i->p} J^T Hbar_i = sum_{p->i} J Hbar_i).
 //
 // Memory: checkpoints every C steps (C ~ sqrt(S)); the backward pass re-runs
-// each segment forward into a segment buffer, then sweeps it backwards.  All
-// vectors are cell-major SoA in global memory, one CTA per trajectory.
+// each segment forward, storing the four stage inputs Y_s of every step, then
+// sweeps it backwards.  A stage VJP is one pass over own cells: the partner's
+// Hbar_p = Y_p x v_p (v = a lam + b Yb_{s+1}, the stage cotangent) is formed
+// from the partner's Y, lam and Yb, and the same Y_p gives the forward field
+// H_i, so neither H nor Hbar is stored.  The bond parameter terms use the bond
+// symmetry (J at the source, J^T at the partner, likewise for dJ/dtheta):
+//   sum_i Hbar_i . DJ_n S_p(n) = sum_p S_p . sum_n DJ_n Hbar_partner(n).
+// A forward stage is one pass that also forms the next stage input and the
+// RK4 sum.  All vectors are cell-major SoA in global memory, one CTA per
+// trajectory.
 #pragma once
 
 #include "rk_global.cuh"
 
 namespace cmd {
+
+// Threads per trajectory CTA.
+constexpr int kAdjThreads = 512;
 
 template <int NAT, int Z, int NQ>
 struct ParamDerivs {
@@ -46,7 +57,7 @@ struct AdjTraj {
     const double* target;      // [S+1][3]
     double* ckpt;              // [K][V] checkpoints (SoA)
     double* seg;               // [C][V] segment buffer
-    double* work;              // 13 * V
+    double* work;              // 5 * V
     double* mloc;              // [S+1][3] M_local of the forward pass
     double* loss;              // [1]
     double* grad;              // [NQ]
@@ -66,118 +77,39 @@ struct AdjArgs {
     int forward_only;
 };
 
-// Forward RK4 over own cells: y <- step(y), stage buffers in w.
+// One fused RK4 stage s (0..3) over own cells, reading the stage input Yin at
+// the neighbours: k = H(Yin, ts) x Yin; H -> Hout when given;
+//   s = 0: acc = k,        Ynext = y + dt/2 k
+//   s = 1: acc = acc + 2k, Ynext = y + dt/2 k
+//   s = 2: acc = acc + 2k, Ynext = y + dt k
+//   s = 3:                 Ynext = y + dt/6 (acc + k)   (Ynext may alias y)
+// which is the RK4 step y + dt/6 (k1 + 2 k2 + 2 k3 + k4) of the reference GPU
+// stepper (integrator.cuh:115-139) summed in the same order.  Only own-cell
+// entries are written, so one barrier after the pass separates the stages.
+// When m is given, the own-cell sum of Yin is added to it.
 template <int NAT, int Z, int LZ>
-__device__ __forceinline__ void rk4_step_global(const Couplings<NAT, Z>& cp, const AdjArgs& a, double* y,
-                                                double* k1, double* k2, double* k3, double* k4, double* Ya,
-                                                double* Yb, double t, double* part) {
+__device__ __forceinline__ void rk4_stage(const Couplings<NAT, Z>& cp, const AdjArgs& a, int s,
+                                          const double* __restrict__ Yin, const double* y, double* acc,
+                                          double* Ynext, double* __restrict__ Hout, double ts, double* m) {
+    constexpr int NL = Z - LZ;
     const int G = a.G, tid = threadIdx.x, nt = blockDim.x;
     const double dt = a.dt;
     const bool drive = a.pulse.a1 != 0.0 || a.pulse.a2 != 0.0;
-    auto rhs = [&](const double* Yin, double* K, double ts, double* pp) {
-        const double f1 = drive ? drive_factor(a.pulse.a1, ts - a.pulse.t1, a.width, a.freq) : 0.0;
-        const double f2 = drive ? drive_factor(a.pulse.a2, ts - a.pulse.t2, a.width, a.freq) : 0.0;
-        for (int g = tid; g < G; g += nt) rhs_cell<NAT, Z, LZ>(cp, Yin, K, G, g, a.nbr, f1, f2, drive, pp);
-    };
-    rhs(y, k1, t, part);
-    __syncthreads();
-    for (int g = tid; g < G; g += nt)
-        for (int e = 0; e < NAT * 3; ++e) {
-            const long long i = (long long)e * G + g;
-            Ya[i] = 1.0 * y[i] + (0.5 * dt) * k1[i];
-        }
-    __syncthreads();
-    rhs(Ya, k2, t + 0.5 * dt, nullptr);
-    for (int g = tid; g < G; g += nt)
-        for (int e = 0; e < NAT * 3; ++e) {
-            const long long i = (long long)e * G + g;
-            Yb[i] = 1.0 * y[i] + (0.5 * dt) * k2[i];
-        }
-    __syncthreads();
-    rhs(Yb, k3, t + 0.5 * dt, nullptr);
-    __syncthreads();
-    for (int g = tid; g < G; g += nt)
-        for (int e = 0; e < NAT * 3; ++e) {
-            const long long i = (long long)e * G + g;
-            Ya[i] = 1.0 * y[i] + dt * k3[i];
-        }
-    __syncthreads();
-    rhs(Ya, k4, t + dt, nullptr);
-    for (int g = tid; g < G; g += nt)
-        for (int e = 0; e < NAT * 3; ++e) {
-            const long long i = (long long)e * G + g;
-            y[i] += (dt / 6.0) * (k1[i] + 2.0 * k2[i] + 2.0 * k3[i] + k4[i]);
-        }
-    __syncthreads();
-}
-
-// Block sum of 3 values (thread 0 gets the totals).
-__device__ __forceinline__ void block_sum3(double (&v)[4], double* red, double* out) {
-    block_sum<4>(v, red, 3, out);
-}
-
-template <int NAT, int Z, int LZ>
-__global__ void __launch_bounds__(256)
-adjoint_forward_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_constant__ AdjArgs a) {
-    __shared__ double red[32 * kRedStride];
-    __shared__ double tot[4];
-    const int b = blockIdx.x;
-    const AdjTraj& T = a.traj[b];
-    const int G = a.G, tid = threadIdx.x, nt = blockDim.x;
-    const long long V = (long long)NAT * 3 * G;
-    double* y = T.work;
-    double* k1 = T.work + V; double* k2 = T.work + 2 * V; double* k3 = T.work + 3 * V; double* k4 = T.work + 4 * V;
-    double* Ya = T.work + 5 * V; double* Yb = T.work + 6 * V;
-    const double N = (double)G * NAT;
-    for (int g = tid; g < G; g += nt)
-        for (int at = 0; at < NAT; ++at)
-            for (int c = 0; c < 3; ++c) y[(at * 3 + c) * G + g] = T.y0[((long long)g * NAT + at) * 3 + c];
-    __syncthreads();
-    double loss = 0.0;
-    for (long long n = 0; n <= a.n_steps; ++n) {
-        if (!a.forward_only && n % a.ckpt_every == 0 && n < a.n_steps) {
-            double* dst = T.ckpt + (n / a.ckpt_every) * V;
-            for (int g = tid; g < G; g += nt)
-                for (int e = 0; e < NAT * 3; ++e) dst[(long long)e * G + g] = y[(long long)e * G + g];
-        }
-        double m[4] = {0, 0, 0, 0};
-        for (int g = tid; g < G; g += nt)
-            for (int at = 0; at < NAT; ++at)
-                for (int c = 0; c < 3; ++c) m[c] += y[(at * 3 + c) * G + g];
-        block_sum3(m, red, tot);
-        if (tid == 0) {
-            for (int c = 0; c < 3; ++c) {
-                const double mc = tot[c] / N;
-                T.mloc[3 * n + c] = mc;
-                const double r = mc - T.target[3 * n + c];
-                loss += r * r;
-            }
-        }
-        __syncthreads();
-        if (n == a.n_steps) break;
-        rk4_step_global<NAT, Z, LZ>(cp, a, y, k1, k2, k3, k4, Ya, Yb, a.times[n], nullptr);
-    }
-    if (tid == 0) T.loss[0] = loss;
-}
-
-// Phase A of a stage VJP over own cells: H (forward field at Y), Hbar = S x v,
-// parameter cotangents.  Writes H and Hbar (SoA).
-template <int NAT, int Z, int LZ, int NQ>
-__device__ __forceinline__ void vjp_phase_a(const Couplings<NAT, Z>& cp, const ParamDerivs<NAT, Z, NQ>& pd,
-                                            const AdjArgs& a, const double* __restrict__ Y,
-                                            const double* __restrict__ v, double* __restrict__ Hout,
-                                            double* __restrict__ Hbar, double ts, double (&gq)[NQ]) {
-    constexpr int NL = Z - LZ;
-    const int G = a.G, tid = threadIdx.x, nt = blockDim.x;
-    const bool drive = a.pulse.a1 != 0.0 || a.pulse.a2 != 0.0;
     const double f1 = drive ? drive_factor(a.pulse.a1, ts - a.pulse.t1, a.width, a.freq) : 0.0;
     const double f2 = drive ? drive_factor(a.pulse.a2, ts - a.pulse.t2, a.width, a.freq) : 0.0;
+    const double cy = s == 2 ? dt : 0.5 * dt;
     for (int g = tid; g < G; g += nt) {
         double S[NAT][3];
 #pragma unroll
         for (int at = 0; at < NAT; ++at)
 #pragma unroll
-            for (int c = 0; c < 3; ++c) S[at][c] = Y[(at * 3 + c) * G + g];
+            for (int c = 0; c < 3; ++c) S[at][c] = Yin[(at * 3 + c) * G + g];
+        if (m) {
+#pragma unroll
+            for (int at = 0; at < NAT; ++at)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) m[c] += S[at][c];
+        }
 #pragma unroll
         for (int at = 0; at < NAT; ++at) {
             double H[3];
@@ -191,109 +123,246 @@ __device__ __forceinline__ void vjp_phase_a(const Couplings<NAT, Z>& cp, const P
                     H[d] += 2.0 * cp.onsite[at][3 * d + 2] * S[at][2];
                 }
             }
-            const double v0 = v[(at * 3 + 0) * G + g], v1 = v[(at * 3 + 1) * G + g], v2 = v[(at * 3 + 2) * G + g];
-            const double hb[3] = {S[at][1] * v2 - S[at][2] * v1, S[at][2] * v0 - S[at][0] * v2,
-                                  S[at][0] * v1 - S[at][1] * v0};
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) {
-                double acc = -(hb[0] * pd.DB[q][at][0] + hb[1] * pd.DB[q][at][1] + hb[2] * pd.DB[q][at][2]);
-                if (pd.has_DA) {
-#pragma unroll
-                    for (int d = 0; d < 3; ++d)
-                        acc += 2.0 * hb[d] * (pd.DA[q][at][3 * d] * S[at][0] + pd.DA[q][at][3 * d + 1] * S[at][1] +
-                                              pd.DA[q][at][3 * d + 2] * S[at][2]);
-                }
-                gq[q] += acc;
-            }
-            auto bond = [&](int n, double P0, double P1, double P2) {
-#pragma unroll
-                for (int d = 0; d < 3; ++d)
-                    H[d] += cp.J[at][n][3 * d] * P0 + cp.J[at][n][3 * d + 1] * P1 + cp.J[at][n][3 * d + 2] * P2;
-#pragma unroll
-                for (int q = 0; q < NQ; ++q) {
-                    const double* D = pd.DJ[q][at][n];
-                    gq[q] += hb[0] * (D[0] * P0 + D[1] * P1 + D[2] * P2) + hb[1] * (D[3] * P0 + D[4] * P1 + D[5] * P2) +
-                             hb[2] * (D[6] * P0 + D[7] * P1 + D[8] * P2);
-                }
-            };
 #pragma unroll
             for (int n = 0; n < LZ; ++n) {
                 const int pb = (at + 1 + n) % NAT;
-                bond(n, S[pb][0], S[pb][1], S[pb][2]);
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    H[d] += cp.J[at][n][3 * d] * S[pb][0] + cp.J[at][n][3 * d + 1] * S[pb][1] +
+                            cp.J[at][n][3 * d + 2] * S[pb][2];
             }
 #pragma unroll
-            for (int m = 0; m < NL; ++m) {
-                const int n = LZ + m;
+            for (int mm = 0; mm < NL; ++mm) {
+                const int n = LZ + mm;
                 if (n < cp.zc[at]) {
-                    const int p = a.nbr[((long long)g * NAT + at) * NL + m];
-                    bond(n, Y[p], Y[p + G], Y[p + 2 * G]);
+                    const int p = a.nbr[((long long)g * NAT + at) * NL + mm];
+                    const double P0 = Yin[p], P1 = Yin[p + G], P2 = Yin[p + 2 * G];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d)
+                        H[d] += cp.J[at][n][3 * d] * P0 + cp.J[at][n][3 * d + 1] * P1 + cp.J[at][n][3 * d + 2] * P2;
                 }
             }
             if (drive) {
 #pragma unroll
                 for (int d = 0; d < 3; ++d) H[d] -= cp.d1[at][d] * f1 + cp.d2[at][d] * f2;
             }
+            if (Hout) {
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                Hout[(at * 3 + d) * G + g] = H[d];
-                Hbar[(at * 3 + d) * G + g] = hb[d];
+                for (int d = 0; d < 3; ++d) Hout[(at * 3 + d) * G + g] = H[d];
+            }
+            const double k[3] = {H[1] * S[at][2] - H[2] * S[at][1], H[2] * S[at][0] - H[0] * S[at][2],
+                                 H[0] * S[at][1] - H[1] * S[at][0]};
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const long long i = (long long)(at * 3 + c) * G + g;
+                const double yi = y[i];
+                if (s == 0) {
+                    acc[i] = k[c];
+                    Ynext[i] = 1.0 * yi + cy * k[c];
+                } else if (s < 3) {
+                    acc[i] = acc[i] + 2.0 * k[c];
+                    Ynext[i] = 1.0 * yi + cy * k[c];
+                } else if (Ynext) {
+                    Ynext[i] = yi + (dt / 6.0) * (acc[i] + k[c]);
+                }
             }
         }
     }
 }
 
-// Phase B: Sbar_i = v_i x H_i + 2 A_i^T Hbar_i + sum_n J_n Hbar_p(n); out += scale * Sbar.
+// Block sum of 3 values (thread 0 gets the totals).
+__device__ __forceinline__ void block_sum3(double (&v)[4], double* red, double* out) {
+    block_sum<4>(v, red, 3, out);
+}
+
 template <int NAT, int Z, int LZ>
-__device__ __forceinline__ void vjp_phase_b(const Couplings<NAT, Z>& cp, const AdjArgs& a,
-                                            const double* __restrict__ v, const double* __restrict__ Hin,
-                                            const double* __restrict__ Hbar, double* __restrict__ Sbar) {
+__global__ void __launch_bounds__(kAdjThreads)
+adjoint_forward_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_constant__ AdjArgs a) {
+    __shared__ double red[32 * kRedStride];
+    __shared__ double tot[4];
+    const int b = blockIdx.x;
+    const AdjTraj& T = a.traj[b];
+    const int G = a.G, tid = threadIdx.x, nt = blockDim.x;
+    const long long V = (long long)NAT * 3 * G;
+    double* y = T.work;
+    double* acc = T.work + V;
+    double* Ya = T.work + 2 * V;
+    double* Yb = T.work + 3 * V;
+    const double N = (double)G * NAT;
+    for (int g = tid; g < G; g += nt)
+        for (int at = 0; at < NAT; ++at)
+            for (int c = 0; c < 3; ++c) y[(at * 3 + c) * G + g] = T.y0[((long long)g * NAT + at) * 3 + c];
+    __syncthreads();
+    double loss = 0.0;
+    auto record = [&](long long n) {     // after block_sum3: thread 0 holds the sums
+        if (tid == 0) {
+            for (int c = 0; c < 3; ++c) {
+                const double mc = tot[c] / N;
+                T.mloc[3 * n + c] = mc;
+                const double r = mc - T.target[3 * n + c];
+                loss += r * r;
+            }
+        }
+    };
+    for (long long n = 0; n < a.n_steps; ++n) {
+        if (!a.forward_only && n % a.ckpt_every == 0) {
+            double* dst = T.ckpt + (n / a.ckpt_every) * V;
+            for (int g = tid; g < G; g += nt)
+                for (int e = 0; e < NAT * 3; ++e) dst[(long long)e * G + g] = y[(long long)e * G + g];
+        }
+        const double t = a.times[n];
+        double m[4] = {0, 0, 0, 0};
+        rk4_stage<NAT, Z, LZ>(cp, a, 0, y, y, acc, Ya, nullptr, t, m);
+        block_sum3(m, red, tot);           // its barrier also ends stage 0
+        record(n);
+        rk4_stage<NAT, Z, LZ>(cp, a, 1, Ya, y, acc, Yb, nullptr, t + 0.5 * a.dt, nullptr);
+        __syncthreads();
+        rk4_stage<NAT, Z, LZ>(cp, a, 2, Yb, y, acc, Ya, nullptr, t + 0.5 * a.dt, nullptr);
+        __syncthreads();
+        rk4_stage<NAT, Z, LZ>(cp, a, 3, Ya, y, acc, y, nullptr, t + a.dt, nullptr);
+        __syncthreads();
+    }
+    double m[4] = {0, 0, 0, 0};
+    for (int g = tid; g < G; g += nt)
+        for (int at = 0; at < NAT; ++at)
+            for (int c = 0; c < 3; ++c) m[c] += y[(at * 3 + c) * G + g];
+    block_sum3(m, red, tot);
+    record(a.n_steps);
+    if (tid == 0) T.loss[0] = loss;
+}
+
+// One stage VJP over own cells at stage input Y (time ts) with cotangent
+// v = ca lam + cb Sprev (Sprev unused when cb == 0):
+//   H_i  = field at Y (static + drive),   Hbar_i = S_i x v_i
+//   Yb_i = v_i x H_i + 2 A_i^T Hbar_i + sum_n J_n Hbar_partner(n)
+//   thetabar_q += Hbar_i . (2 DA_q S_i - DB_q) + S_i . sum_n DJ_q,n Hbar_partner(n)
+// then per own entry  mode 0: Sout = Yb, acc = lam + Yb;  mode 1: Sout = Yb,
+// acc += Yb;  mode 2: lam_out = acc + Yb + dl (dl: the loss cotangent at this
+// step, per component).  lam, Sprev and Y are read at the partners, so
+// lam_out and Sout must be other buffers.
+template <int NAT, int Z, int LZ, int NQ>
+__device__ __forceinline__ void stage_vjp(const Couplings<NAT, Z>& cp, const ParamDerivs<NAT, Z, NQ>& pd,
+                                          const AdjArgs& a, const double* __restrict__ Y,
+                                          const double* __restrict__ lam, const double* __restrict__ Sprev,
+                                          double ca, double cb, double ts, double* __restrict__ Sout,
+                                          double* __restrict__ acc, double* __restrict__ lam_out, int mode,
+                                          const double* dl, double (&gq)[NQ]) {
     constexpr int NL = Z - LZ;
     const int G = a.G, tid = threadIdx.x, nt = blockDim.x;
+    const bool drive = a.pulse.a1 != 0.0 || a.pulse.a2 != 0.0;
+    const double f1 = drive ? drive_factor(a.pulse.a1, ts - a.pulse.t1, a.width, a.freq) : 0.0;
+    const double f2 = drive ? drive_factor(a.pulse.a2, ts - a.pulse.t2, a.width, a.freq) : 0.0;
+    auto cot = [&](long long i0, double (&v)[3]) {
+        v[0] = ca * lam[i0];
+        v[1] = ca * lam[i0 + G];
+        v[2] = ca * lam[i0 + 2 * G];
+        if (cb != 0.0) {
+            v[0] = v[0] + cb * Sprev[i0];
+            v[1] = v[1] + cb * Sprev[i0 + G];
+            v[2] = v[2] + cb * Sprev[i0 + 2 * G];
+        }
+    };
+    // spin P and Hbar Q of the site at SoA offset p (own site or partner)
+    auto partner = [&](long long p, double (&P)[3], double (&Q)[3]) {
+        P[0] = Y[p];
+        P[1] = Y[p + G];
+        P[2] = Y[p + 2 * G];
+        double v[3];
+        cot(p, v);
+        Q[0] = P[1] * v[2] - P[2] * v[1];
+        Q[1] = P[2] * v[0] - P[0] * v[2];
+        Q[2] = P[0] * v[1] - P[1] * v[0];
+    };
     for (int g = tid; g < G; g += nt) {
-        double Hb[NAT][3];
-#pragma unroll
-        for (int at = 0; at < NAT; ++at)
-#pragma unroll
-            for (int c = 0; c < 3; ++c) Hb[at][c] = Hbar[(at * 3 + c) * G + g];
-#pragma unroll
+#pragma unroll 1
         for (int at = 0; at < NAT; ++at) {
-            const double v0 = v[(at * 3 + 0) * G + g], v1 = v[(at * 3 + 1) * G + g], v2 = v[(at * 3 + 2) * G + g];
-            const double H0 = Hin[(at * 3 + 0) * G + g], H1 = Hin[(at * 3 + 1) * G + g],
-                         H2 = Hin[(at * 3 + 2) * G + g];
-            double sb[3] = {v1 * H2 - v2 * H1, v2 * H0 - v0 * H2, v0 * H1 - v1 * H0};
+            const long long i0 = (long long)(at * 3) * G + g;
+            double Sown[3], hown[3];
+            partner(i0, Sown, hown);
+            const double S0 = Sown[0], S1 = Sown[1], S2 = Sown[2];
+            double H[3], sb[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int d = 0; d < 3; ++d) H[d] = cp.has_field ? -cp.field[at][d] : 0.0;
             if (cp.has_onsite) {
 #pragma unroll
-                for (int d = 0; d < 3; ++d)
-                    sb[d] += 2.0 * (cp.onsite[at][d] * Hb[at][0] + cp.onsite[at][3 + d] * Hb[at][1] +
-                                    cp.onsite[at][6 + d] * Hb[at][2]);
+                for (int d = 0; d < 3; ++d) {
+                    H[d] += 2.0 * cp.onsite[at][3 * d + 0] * S0;
+                    H[d] += 2.0 * cp.onsite[at][3 * d + 1] * S1;
+                    H[d] += 2.0 * cp.onsite[at][3 * d + 2] * S2;
+                    sb[d] += 2.0 * (cp.onsite[at][d] * hown[0] + cp.onsite[at][3 + d] * hown[1] +
+                                    cp.onsite[at][6 + d] * hown[2]);
+                }
             }
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) {
+                double t = -(hown[0] * pd.DB[q][at][0] + hown[1] * pd.DB[q][at][1] + hown[2] * pd.DB[q][at][2]);
+                if (pd.has_DA) {
+#pragma unroll
+                    for (int d = 0; d < 3; ++d)
+                        t += 2.0 * hown[d] * (pd.DA[q][at][3 * d] * S0 + pd.DA[q][at][3 * d + 1] * S1 +
+                                              pd.DA[q][at][3 * d + 2] * S2);
+                }
+                gq[q] += t;
+            }
+            // bond n with partner spin P and partner Hbar Q
+            auto bond = [&](int n, const double (&P)[3], const double (&Q)[3]) {
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    H[d] += cp.J[at][n][3 * d] * P[0] + cp.J[at][n][3 * d + 1] * P[1] + cp.J[at][n][3 * d + 2] * P[2];
+                    sb[d] += cp.J[at][n][3 * d] * Q[0] + cp.J[at][n][3 * d + 1] * Q[1] + cp.J[at][n][3 * d + 2] * Q[2];
+                }
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) {
+                    const double* D = pd.DJ[q][at][n];
+                    gq[q] += S0 * (D[0] * Q[0] + D[1] * Q[1] + D[2] * Q[2]) +
+                             S1 * (D[3] * Q[0] + D[4] * Q[1] + D[5] * Q[2]) +
+                             S2 * (D[6] * Q[0] + D[7] * Q[1] + D[8] * Q[2]);
+                }
+            };
 #pragma unroll
             for (int n = 0; n < LZ; ++n) {
                 const int pb = (at + 1 + n) % NAT;
-#pragma unroll
-                for (int d = 0; d < 3; ++d)
-                    sb[d] += cp.J[at][n][3 * d] * Hb[pb][0] + cp.J[at][n][3 * d + 1] * Hb[pb][1] +
-                             cp.J[at][n][3 * d + 2] * Hb[pb][2];
+                double P[3], Q[3];
+                partner((long long)(pb * 3) * G + g, P, Q);
+                bond(n, P, Q);
             }
 #pragma unroll
             for (int m = 0; m < NL; ++m) {
                 const int n = LZ + m;
                 if (n < cp.zc[at]) {
-                    const int p = a.nbr[((long long)g * NAT + at) * NL + m];
-                    const double P0 = Hbar[p], P1 = Hbar[p + G], P2 = Hbar[p + 2 * G];
-#pragma unroll
-                    for (int d = 0; d < 3; ++d)
-                        sb[d] += cp.J[at][n][3 * d] * P0 + cp.J[at][n][3 * d + 1] * P1 + cp.J[at][n][3 * d + 2] * P2;
+                    double P[3], Q[3];
+                    partner(a.nbr[((long long)g * NAT + at) * NL + m], P, Q);
+                    bond(n, P, Q);
                 }
             }
+            if (drive) {
 #pragma unroll
-            for (int d = 0; d < 3; ++d) Sbar[(at * 3 + d) * G + g] = sb[d];
+                for (int d = 0; d < 3; ++d) H[d] -= cp.d1[at][d] * f1 + cp.d2[at][d] * f2;
+            }
+            double v[3];
+            cot(i0, v);
+            sb[0] += v[1] * H[2] - v[2] * H[1];
+            sb[1] += v[2] * H[0] - v[0] * H[2];
+            sb[2] += v[0] * H[1] - v[1] * H[0];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const long long i = i0 + d * G;
+                if (mode == 0) {
+                    Sout[i] = sb[d];
+                    acc[i] = lam[i] + sb[d];
+                } else if (mode == 1) {
+                    Sout[i] = sb[d];
+                    acc[i] = acc[i] + sb[d];
+                } else {
+                    lam_out[i] = acc[i] + sb[d] + dl[d];
+                }
+            }
         }
     }
 }
 
 template <int NAT, int Z, int LZ, int NQ>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kAdjThreads)
 adjoint_backward_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_constant__ ParamDerivs<NAT, Z, NQ> pd,
                         const __grid_constant__ AdjArgs a) {
     __shared__ double red[32 * kRedStride];
@@ -302,15 +371,11 @@ adjoint_backward_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __gr
     const AdjTraj& T = a.traj[b];
     const int G = a.G, tid = threadIdx.x, nt = blockDim.x;
     const long long V = (long long)NAT * 3 * G;
-    double* y = T.work;
-    double* k1 = T.work + 1 * V; double* k2 = T.work + 2 * V; double* k3 = T.work + 3 * V;
-    double* Y2 = T.work + 4 * V; double* Y3 = T.work + 5 * V; double* Y4 = T.work + 6 * V;
-    double* lam = T.work + 7 * V;
-    double* kb = T.work + 8 * V;
-    double* Hs = T.work + 9 * V;
-    double* Hb = T.work + 10 * V;
-    double* Sb = T.work + 11 * V;
-    double* tmp = T.work + 12 * V;
+    double* lam = T.work;               // cotangent of y_{n+1}; lam2 receives that of y_n
+    double* lam2 = T.work + 1 * V;
+    double* acc = T.work + 2 * V;       // RK4 sum (recompute) / ybar accumulator (sweep)
+    double* Sa = T.work + 3 * V;
+    double* Sb = T.work + 4 * V;
     const double N = (double)G * NAT;
     const double dt = a.dt;
     const long long S = a.n_steps;
@@ -319,102 +384,62 @@ adjoint_backward_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __gr
     for (int q = 0; q < NQ; ++q) gq[q] = 0.0;
 
     auto dl = [&](long long n, int c) { return 2.0 * (T.mloc[3 * n + c] - T.target[3 * n + c]) / N; };
-    // lam_S = dl_S/dy_S (uniform over sites)
     for (int g = tid; g < G; g += nt)
         for (int at = 0; at < NAT; ++at)
             for (int c = 0; c < 3; ++c) lam[(at * 3 + c) * G + g] = dl(S, c);
     __syncthreads();
-    const bool drive = a.pulse.a1 != 0.0 || a.pulse.a2 != 0.0;
-    auto rhs = [&](const double* Yin, double* K, double ts) {
-        const double f1 = drive ? drive_factor(a.pulse.a1, ts - a.pulse.t1, a.width, a.freq) : 0.0;
-        const double f2 = drive ? drive_factor(a.pulse.a2, ts - a.pulse.t2, a.width, a.freq) : 0.0;
-        for (int g = tid; g < G; g += nt) rhs_cell<NAT, Z, LZ>(cp, Yin, K, G, g, a.nbr, f1, f2, drive, nullptr);
-    };
-    // one stage VJP: Sb = f_Y(Ystage)^T v
-    auto stage_vjp = [&](const double* Ystage, const double* v, double ts) {
-        vjp_phase_a<NAT, Z, LZ, NQ>(cp, pd, a, Ystage, v, Hs, Hb, ts, gq);
-        __syncthreads();
-        vjp_phase_b<NAT, Z, LZ>(cp, a, v, Hs, Hb, Sb);
-        __syncthreads();
-    };
+    // Segment slot layout: step j of the segment holds [Y1 Y2 Y3 Y4].
+    auto slot = [&](long long j, int q) { return T.seg + (j * 4 + q) * V; };
     const long long C = a.ckpt_every;
     const long long K = (S + C - 1) / C;
     for (long long seg = K - 1; seg >= 0; --seg) {
         const long long n0 = seg * C;
         const long long n1 = (n0 + C < S) ? n0 + C : S;
-        // re-run the segment forward from its checkpoint, storing y_n
-        for (int g = tid; g < G; g += nt)
-            for (int e = 0; e < NAT * 3; ++e) y[(long long)e * G + g] = T.ckpt[seg * V + (long long)e * G + g];
-        __syncthreads();
-        for (long long n = n0; n < n1; ++n) {
-            double* dst = T.seg + (n - n0) * V;
+        // forward recompute of the segment from its checkpoint, keeping every
+        // stage input of every step
+        {
+            double* y1 = slot(0, 0);
             for (int g = tid; g < G; g += nt)
-                for (int e = 0; e < NAT * 3; ++e) dst[(long long)e * G + g] = y[(long long)e * G + g];
-            if (n + 1 < n1) rk4_step_global<NAT, Z, LZ>(cp, a, y, k1, k2, k3, Hs, Y2, Y3, a.times[n], nullptr);
+                for (int e = 0; e < NAT * 3; ++e) y1[(long long)e * G + g] = T.ckpt[seg * V + (long long)e * G + g];
         }
         __syncthreads();
-        for (long long n = n1 - 1; n >= n0; --n) {
+        for (long long n = n0; n < n1; ++n) {
+            const long long j = n - n0;
             const double t = a.times[n];
-            const double* yn = T.seg + (n - n0) * V;
-            // stage inputs of step n
-            rhs(yn, k1, t);
+            double* y = slot(j, 0);
+            rk4_stage<NAT, Z, LZ>(cp, a, 0, y, y, acc, slot(j, 1), nullptr, t, nullptr);
             __syncthreads();
-            for (int g = tid; g < G; g += nt)
-                for (int e = 0; e < NAT * 3; ++e) {
-                    const long long i = (long long)e * G + g;
-                    Y2[i] = 1.0 * yn[i] + (0.5 * dt) * k1[i];
-                }
+            rk4_stage<NAT, Z, LZ>(cp, a, 1, slot(j, 1), y, acc, slot(j, 2), nullptr, t + 0.5 * dt, nullptr);
             __syncthreads();
-            rhs(Y2, k2, t + 0.5 * dt);
+            rk4_stage<NAT, Z, LZ>(cp, a, 2, slot(j, 2), y, acc, slot(j, 3), nullptr, t + 0.5 * dt, nullptr);
             __syncthreads();
-            for (int g = tid; g < G; g += nt)
-                for (int e = 0; e < NAT * 3; ++e) {
-                    const long long i = (long long)e * G + g;
-                    Y3[i] = 1.0 * yn[i] + (0.5 * dt) * k2[i];
-                }
+            rk4_stage<NAT, Z, LZ>(cp, a, 3, slot(j, 3), y, acc, n + 1 < n1 ? slot(j + 1, 0) : nullptr, nullptr,
+                                  t + dt, nullptr);
             __syncthreads();
-            rhs(Y3, k3, t + 0.5 * dt);
+        }
+        for (long long n = n1 - 1; n >= n0; --n) {
+            const long long j = n - n0;
+            const double t = a.times[n];
+            // stage 4: kb4 = dt/6 lam -> Yb4 (Sa); acc = lam + Yb4
+            stage_vjp<NAT, Z, LZ, NQ>(cp, pd, a, slot(j, 3), lam, nullptr, dt / 6.0, 0.0, t + dt, Sa, acc, nullptr,
+                                      0, nullptr, gq);
             __syncthreads();
-            for (int g = tid; g < G; g += nt)
-                for (int e = 0; e < NAT * 3; ++e) {
-                    const long long i = (long long)e * G + g;
-                    Y4[i] = 1.0 * yn[i] + dt * k3[i];
-                    kb[i] = (dt / 6.0) * lam[i];                 // kbar4
-                    tmp[i] = lam[i];                             // ybar accumulator
-                }
+            // stage 3: kb3 = dt/3 lam + dt Yb4 -> Yb3 (Sb); acc += Yb3
+            stage_vjp<NAT, Z, LZ, NQ>(cp, pd, a, slot(j, 2), lam, Sa, dt / 3.0, dt, t + 0.5 * dt, Sb, acc, nullptr,
+                                      1, nullptr, gq);
             __syncthreads();
-            stage_vjp(Y4, kb, t + dt);                           // Sb = Yb4
-            for (int g = tid; g < G; g += nt)
-                for (int e = 0; e < NAT * 3; ++e) {
-                    const long long i = (long long)e * G + g;
-                    tmp[i] += Sb[i];
-                    kb[i] = (dt / 3.0) * lam[i] + dt * Sb[i];    // kbar3
-                }
+            // stage 2: kb2 = dt/3 lam + dt/2 Yb3 -> Yb2 (Sa); acc += Yb2
+            stage_vjp<NAT, Z, LZ, NQ>(cp, pd, a, slot(j, 1), lam, Sb, dt / 3.0, 0.5 * dt, t + 0.5 * dt, Sa, acc,
+                                      nullptr, 1, nullptr, gq);
             __syncthreads();
-            stage_vjp(Y3, kb, t + 0.5 * dt);                     // Sb = Yb3
-            for (int g = tid; g < G; g += nt)
-                for (int e = 0; e < NAT * 3; ++e) {
-                    const long long i = (long long)e * G + g;
-                    tmp[i] += Sb[i];
-                    kb[i] = (dt / 3.0) * lam[i] + (0.5 * dt) * Sb[i];   // kbar2
-                }
+            // stage 1: kb1 = dt/6 lam + dt/2 Yb2 -> Yb1; lam_n = acc + Yb1 + dl_n
+            const double dln[3] = {dl(n, 0), dl(n, 1), dl(n, 2)};
+            stage_vjp<NAT, Z, LZ, NQ>(cp, pd, a, slot(j, 0), lam, Sa, dt / 6.0, 0.5 * dt, t, nullptr, acc, lam2, 2,
+                                      dln, gq);
             __syncthreads();
-            stage_vjp(Y2, kb, t + 0.5 * dt);                     // Sb = Yb2
-            for (int g = tid; g < G; g += nt)
-                for (int e = 0; e < NAT * 3; ++e) {
-                    const long long i = (long long)e * G + g;
-                    tmp[i] += Sb[i];
-                    kb[i] = (dt / 6.0) * lam[i] + (0.5 * dt) * Sb[i];   // kbar1
-                }
-            __syncthreads();
-            stage_vjp(yn, kb, t);                                // Sb = Yb1
-            for (int g = tid; g < G; g += nt)
-                for (int at = 0; at < NAT; ++at)
-                    for (int c = 0; c < 3; ++c) {
-                        const long long i = (long long)(at * 3 + c) * G + g;
-                        lam[i] = tmp[i] + Sb[i] + dl(n, c);
-                    }
-            __syncthreads();
+            double* sw = lam;
+            lam = lam2;
+            lam2 = sw;
         }
     }
     double v[16];
