@@ -81,6 +81,7 @@ _SIGS = {
     "cmd_run_batch": (C.c_int, [C.c_void_p, C.POINTER(BatchDesc)]),
     "cmd_batch_rows": (C.c_int64, [C.c_int64, C.c_int64]),
     "cmd_run_batch_device": (C.c_int, [C.c_void_p, C.POINTER(BatchDesc), C.c_void_p, _I32]),
+    "cmd_run_batch_device_noalloc": (C.c_int, [C.c_void_p, C.POINTER(BatchDesc), C.c_void_p, _I32]),
     "cmd_layout_info": (C.c_int, [C.c_void_p, _I64]),
     "cmd_plan_layout": (C.c_int, [C.POINTER(LatticeDesc), _I64]),
     "cmd_run_uneven": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.c_double, C.c_double, C.c_int64]),

@@ -179,6 +179,30 @@ int64_t cmd_batch_rows(int64_t n_steps, int64_t save_interval);
  */
 int cmd_run_batch_device(cmd_handle* h, const cmd_batch_desc* d, void* stream, int32_t* launches);
 
+/*
+ * Allocation-free variant of cmd_run_batch_device.  It has no counterpart in
+ * the reference.  It is for callers that cannot call cudaMalloc: their device
+ * memory already belongs to another allocator (a caching allocator that has
+ * reserved the GPU, a pre-partitioned serving pool), or they run loops that
+ * cannot take the device-wide synchronisation cudaMalloc / cudaFree may imply.
+ * Same arguments and results as cmd_run_batch_device, and the same kernels.
+ * The scratch that cmd_run_batch_device allocates on demand lives here in one
+ * static device array of 2^22 doubles (32 MiB), which every GPU that loads
+ * this library holds until the process exits:
+ *     scratch doubles = [driven] n_steps + B*n_steps*6
+ *                     + [cells of more than 3 atoms] B*rows*(3*atoms+1)
+ * (each term rounded up to a multiple of 32).  A batch needing more is
+ * rejected with CMD_ERR_INVALID_ARG; split it into smaller batches.
+ * The call allocates no device memory.  Its first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture.  Every call
+ * shares the one array, so calls whose work overlaps on the GPU (other
+ * streams, other handles, other threads) race: order them on one stream, or
+ * synchronise between them.  Everything a call reads from the array it first
+ * writes itself, so nothing carries over between calls.
+ */
+int cmd_run_batch_device_noalloc(cmd_handle* h, const cmd_batch_desc* d, void* stream, int32_t* launches);
+
 /* Lattice layout chosen at cmd_create (for diagnostics and the autotuner):
  * info[0] = sites per group (unit-cell atoms), info[1] = groups,
  * info[2] = max bonds per site kept, info[3] = threads per block of the
