@@ -14,6 +14,7 @@
 #include "rk4_resident.cuh"
 #include "rk_global.cuh"
 #include "rk_adjoint.cuh"
+#include "rk_stream.cuh"
 
 #include <cuda_runtime.h>
 
@@ -104,6 +105,7 @@ struct cmd_handle {
     DevBuf dframes, dafm, times, drive, raw, tune_states, tune_obs;
     DevBuf gwork, gmeta, gstat, grows, gqueue;
     DevBuf awork, ackpt, aseg, amloc, aout, ameta, ain;
+    DevBuf sbuf, spart, sgpart;  // streamed RK4 / adjoint: stage vectors, tile partials
     bool has_state = false;
     int variant = -1;           // resident-kernel variant; -1 = heuristic default
     // pulse (set_gpu_pulse)
@@ -492,6 +494,115 @@ int run_resident(cmd_handle* h, const RunSpec& r, cudaStream_t st, int32_t* laun
 }
 
 // ---------------------------------------------------------------------------
+// Streamed RK4 (rk_stream.cuh): lattices no resident variant holds.  One launch
+// per stage over (cell tile, trajectory); same RunSpec contract and outputs as
+// run_resident.
+
+template <int NAT, int Z, int LZ>
+int stream_forward(cmd_handle* h, const RunSpec& r, cudaStream_t st, int32_t* launches) {
+    constexpr int NR = 3 * NAT + 1;
+    int32_t nl = 0;
+    const int G = (int)h->lay.G;
+    const int tiles = (G + cmd::kStreamTile - 1) / cmd::kStreamTile;
+    const int64_t V = (int64_t)NAT * 3 * G;
+    const int64_t B = r.B;
+    if (B > 65535) return fail(CMD_ERR_UNSUPPORTED, "streamed batches are limited to 65535 trajectories");
+    if (r.traj && B != 1) return fail(CMD_ERR_UNSUPPORTED, "streamed state saving is for single trajectories");
+    const int64_t rows = rows_for(r.n_steps, r.save);
+    if (int rc = h->sbuf.ensure((size_t)4 * B * V * sizeof(double))) return rc;
+    if (int rc = h->spart.ensure((size_t)B * tiles * cmd::kPart * sizeof(double))) return rc;
+    double* base = h->sbuf.as<double>();
+    const cmd::SVec y{base, V}, acc{base + B * V, V}, Ya{base + 2 * B * V, V}, Yb{base + 3 * B * V, V};
+    cmd::StreamArgs a{};
+    a.G = G;
+    a.tiles = tiles;
+    a.B = (int)B;
+    a.nbr = h->nbr.as<int>();
+    a.dt = r.dt;
+    a.n_steps = r.n_steps;
+    a.part = h->spart.as<double>();
+    a.n_sites = r.n_sites;
+    a.save_every = r.save;
+    a.rows = rows;
+    a.V = V;
+    if (r.obs) {
+        if (NR <= 10) {
+            a.raw = r.obs;
+            a.raw_stride = 10;
+        } else {
+            if (int rc = h->raw.ensure((size_t)B * rows * NR * sizeof(double))) return rc;
+            a.raw = h->raw.as<double>();
+            a.raw_stride = NR;
+        }
+    }
+    if (r.pulses && r.n_steps > 0) {
+        std::vector<double> grid;
+        grid.reserve(r.n_steps);
+        double t = r.T0;
+        for (int64_t k = 0; k < r.n_steps; ++k) {     // t_k of the reference loop (t += dt)
+            grid.push_back(t);
+            t += r.dt;
+        }
+        if (int rc = h->times.ensure(grid.size() * sizeof(double))) return rc;
+        if (int rc = h->drive.ensure((size_t)B * r.n_steps * 6 * sizeof(double))) return rc;
+        CUDA_TRY(cudaMemcpyAsync(h->times.p, grid.data(), grid.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+        const int64_t total = B * r.n_steps * 6;
+        const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 32);
+        cmd::drive_table_kernel<<<blocks, 256, 0, st>>>(r.pulses, h->times.as<double>(), r.n_steps, r.dt, r.width,
+                                                       r.freq, B, h->drive.as<double>());
+        CUDA_TRY(cudaGetLastError());
+        ++nl;
+        a.times = h->times.as<double>();
+        a.drive = h->drive.as<double>();
+    }
+    static const std::vector<double> zeros(3 * 64, 0.0);
+    cmd::Couplings<NAT, Z> cp;
+    fill_couplings<NAT, Z>(h, r.d1 ? r.d1 : zeros.data(), r.d2 ? r.d2 : zeros.data(), cp);
+    const dim3 grid(tiles, (unsigned)B), gridc((G + 255) / 256, (unsigned)B);
+    const int64_t N3 = (int64_t)G * NAT * 3;
+    auto save_traj = [&](int64_t row) {
+        const cmd::SVec src = y;
+        cmd::stream_store_kernel<NAT><<<gridc, 256, 0, st>>>(src, G, r.traj + row * N3);
+        ++nl;
+    };
+    cmd::stream_load_kernel<NAT><<<gridc, 256, 0, st>>>(r.y0, r.y0_stride, G, y);
+    CUDA_TRY(cudaGetLastError());
+    ++nl;
+    const int with_obs = r.obs ? 1 : 0;
+    for (int64_t n = 0; n < r.n_steps; ++n) {
+        if (r.traj && n % r.save == 0) save_traj(n / r.save);
+        cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 0, n, y, y, acc, Ya, with_obs);
+        cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 1, n, Ya, y, acc, Yb, with_obs);
+        cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 2, n, Yb, y, acc, Ya, with_obs);
+        cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 3, n, Ya, y, acc, y, with_obs);
+        nl += 4;
+        if ((n & 1023) == 0) CUDA_TRY(cudaGetLastError());
+    }
+    CUDA_TRY(cudaGetLastError());
+    if (r.traj) save_traj(rows - 1);
+    if (r.obs) {
+        cmd::stream_obs_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, y);
+        cmd::stream_reduce_kernel<NAT><<<(unsigned)B, cmd::kStreamTile, 0, st>>>(a, r.n_steps);
+        CUDA_TRY(cudaGetLastError());
+        nl += 2;
+    }
+    if (r.y_out) {
+        cmd::stream_store_kernel<NAT><<<gridc, 256, 0, st>>>(y, G, r.y_out);
+        CUDA_TRY(cudaGetLastError());
+        ++nl;
+    }
+    if (r.obs) {
+        const double* fr = r.frames ? r.frames : h->dframes.as<double>();
+        const double* af = r.afm ? r.afm : h->dafm.as<double>();
+        launch_finish<NAT>(a.raw, a.raw_stride, B * rows, fr, af, r.n_sites, r.obs, st);
+        CUDA_TRY(cudaGetLastError());
+        ++nl;
+    }
+    if (launches) *launches = nl;
+    return CMD_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Global-state integrator (rk_global.cuh): controlled / fixed Dormand-Prince and
 // global-memory RK4, persistent over a queue of trajectories.
 
@@ -506,6 +617,17 @@ int global_type(const Layout& L) {
 }
 
 bool layout_has_kernel(const Layout& L) { return default_variant(L) >= 0 || global_type(L) >= 0; }
+
+// RK4 over the handle's lattice: the resident kernel when a variant holds the
+// lattice (or one is named), else the streamed stage kernels.
+int run_rk4(cmd_handle* h, const RunSpec& r, cudaStream_t st, int32_t* launches) {
+    if (r.variant >= 0 || pick_variant(h) >= 0) return run_resident(h, r, st, launches);
+    switch (global_type(h->lay)) {
+        case 0: return stream_forward<2, 3, 1>(h, r, st, launches);
+        case 1: return stream_forward<4, 6, 3>(h, r, st, launches);
+        default: return no_instance(h->lay);
+    }
+}
 
 struct GJob {
     cmd_handle* h = nullptr;
@@ -785,7 +907,8 @@ int cmd_destroy(cmd_handle* h) {
     for (DevBuf* b : {&h->state, &h->nbr, &h->obs, &h->traj, &h->batch_states, &h->batch_out,
                       &h->pulses, &h->scratch, &h->dframes, &h->dafm, &h->times, &h->drive, &h->raw,
                       &h->tune_states, &h->tune_obs, &h->gwork, &h->gmeta, &h->gstat, &h->grows, &h->gqueue,
-                      &h->awork, &h->ackpt, &h->aseg, &h->amloc, &h->aout, &h->ameta, &h->ain})
+                      &h->awork, &h->ackpt, &h->aseg, &h->amloc, &h->aout, &h->ameta, &h->ain,
+                      &h->sbuf, &h->spart, &h->sgpart})
         b->release();
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -876,7 +999,7 @@ int run_single(cmd_handle* h, double T0, double dt, int64_t n_steps, int64_t sav
     r.d1 = h->fd.data();
     r.d2 = h->fd.data() + 3 * h->NA;
     r.n_sites = n_sites;
-    if (int rc = run_resident(h, r, h->stream, nullptr)) return rc;
+    if (int rc = run_rk4(h, r, h->stream, nullptr)) return rc;
     return sync(h);
 }
 
@@ -915,6 +1038,7 @@ int run_global_single(cmd_handle* h, int method, double T0, double T1, double dt
 }
 
 bool resident_fits(const cmd_handle* h) { return pick_variant(h) >= 0; }
+bool rk4_fits(const cmd_handle* h) { return resident_fits(h) || global_type(h->lay) >= 0; }
 
 }  // namespace
 
@@ -961,7 +1085,7 @@ int cmd_integrate(cmd_handle* h, double T0, double T1, double dt, int64_t save_i
     const int64_t rows = rows_for(n, save_interval);
     if (rows_out) *rows_out = rows;
     if (max_rows < rows) return fail(CMD_ERR_INVALID_ARG, "max_rows too small");
-    if (method == CMD_RK4 && resident_fits(h)) {
+    if (method == CMD_RK4 && rk4_fits(h)) {
         if (int rc = run_single(h, T0, dt, n, save_interval, (double)h->N, obs != nullptr, states != nullptr, true))
             return rc;
         if (obs) CUDA_TRY(cudaMemcpy(obs, h->obs.p, rows * 10 * sizeof(double), cudaMemcpyDeviceToHost));
@@ -1139,7 +1263,7 @@ int run_batch_device(cmd_handle* h, const cmd_batch_desc* d, const cmd::Pulse* d
     r.d1 = d->d1 ? d1c.data() : nullptr;
     r.d2 = d->d2 ? d2c.data() : nullptr;
     r.n_sites = (double)h->N;
-    return run_resident(h, r, st, launches);
+    return run_rk4(h, r, st, launches);
 }
 
 }  // namespace
@@ -1220,6 +1344,155 @@ int launch_adjoint(cmd_handle* h, const cmd::AdjArgs& a, const std::vector<doubl
         }
     pd.has_DA = has_DA;
     cmd::adjoint_backward_kernel<NAT, Z, LZ, kAdjParams><<<(unsigned)B, cmd::kAdjThreads, 0, h->stream>>>(cp, pd, a);
+    CUDA_TRY(cudaGetLastError());
+    return CMD_OK;
+}
+
+
+// Streamed adjoint (rk_stream.cuh) for batches too small to fill the GPU with
+// one CTA per trajectory: every stage (forward, recompute, VJP) is one launch
+// over (cell tile, trajectory).
+struct StreamAdjJob {
+    int64_t B, S, C, K;
+    bool fwd_only;
+    const double* y0;          // device AoS [B][N*3]
+    const double* target;      // device [B][S+1][3]
+    const double* times;       // device [S+1]
+    double* mloc;              // device [B][S+1][3]
+    double* out;               // device [B][1 + kAdjParams]: loss, grad
+    double dt;
+};
+
+template <int NAT, int Z, int LZ>
+int stream_adjoint(cmd_handle* h, const StreamAdjJob& j, const std::vector<double>& DJ, const std::vector<double>& DB,
+                   const std::vector<double>& DA, bool has_DA) {
+    cudaStream_t st = h->stream;
+    const int G = (int)h->lay.G;
+    const int tiles = (G + cmd::kStreamTile - 1) / cmd::kStreamTile;
+    const int64_t V = (int64_t)NAT * 3 * G, B = j.B, S = j.S, C = j.C, K = j.K;
+    if (int rc = h->sbuf.ensure((size_t)5 * B * V * sizeof(double))) return rc;
+    if (int rc = h->spart.ensure(((size_t)B * tiles * cmd::kPart + B) * sizeof(double))) return rc;
+    if (int rc = h->sgpart.ensure((size_t)B * tiles * cmd::kPart * sizeof(double))) return rc;
+    double* base = h->sbuf.as<double>();
+    double* d_loss = h->spart.as<double>() + (size_t)B * tiles * cmd::kPart;
+    const bool driven = h->amp != 0.0;
+    if (driven) {
+        std::vector<cmd::Pulse> pl((size_t)B, cmd::Pulse{h->t1, h->t2, h->amp, h->amp});
+        if (int rc = h->pulses.ensure((size_t)B * sizeof(cmd::Pulse))) return rc;
+        if (int rc = h->drive.ensure((size_t)B * S * 6 * sizeof(double))) return rc;
+        CUDA_TRY(cudaMemcpyAsync(h->pulses.p, pl.data(), pl.size() * sizeof(cmd::Pulse), cudaMemcpyHostToDevice, st));
+        const int64_t total = B * S * 6;
+        const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 32);
+        cmd::drive_table_kernel<<<blocks, 256, 0, st>>>(h->pulses.as<cmd::Pulse>(), j.times, S, j.dt, h->width,
+                                                       h->freq, B, h->drive.as<double>());
+        CUDA_TRY(cudaGetLastError());
+    }
+    cmd::Couplings<NAT, Z> cp;
+    fill_couplings<NAT, Z>(h, h->fd.data(), h->fd.data() + 3 * h->NA, cp);
+    cmd::StreamArgs a{};
+    a.G = G;
+    a.tiles = tiles;
+    a.B = (int)B;
+    a.nbr = h->nbr.as<int>();
+    a.dt = j.dt;
+    a.n_steps = S;
+    a.times = j.times;
+    a.drive = driven ? h->drive.as<double>() : nullptr;
+    a.part = h->spart.as<double>();
+    a.save_every = 1;
+    a.rows = S + 1;
+    a.target = j.target;
+    a.mloc = j.mloc;
+    a.loss = d_loss;
+    a.n_sites = (double)h->N;
+    a.ckpt = j.fwd_only ? nullptr : h->ackpt.as<double>();
+    a.ckpt_every = C;
+    a.n_ckpt = K;
+    a.V = V;
+    const dim3 grid(tiles, (unsigned)B), gridc((G + 255) / 256, (unsigned)B);
+    const cmd::SVec none{nullptr, 0};
+    // forward: loss terms every step, checkpoints every C steps
+    {
+        const cmd::SVec y{base, V}, acc{base + B * V, V}, Ya{base + 2 * B * V, V}, Yb{base + 3 * B * V, V};
+        cmd::stream_load_kernel<NAT><<<gridc, 256, 0, st>>>(j.y0, (long long)G * NAT * 3, G, y);
+        for (int64_t n = 0; n < S; ++n) {
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 0, n, y, y, acc, Ya, 1);
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 1, n, Ya, y, acc, Yb, 1);
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 2, n, Yb, y, acc, Ya, 1);
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 3, n, Ya, y, acc, y, 1);
+            if ((n & 1023) == 0) CUDA_TRY(cudaGetLastError());
+        }
+        cmd::stream_obs_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, y);
+        cmd::stream_reduce_kernel<NAT><<<(unsigned)B, cmd::kStreamTile, 0, st>>>(a, S);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemcpy2DAsync(j.out, (1 + kAdjParams) * sizeof(double), d_loss, sizeof(double), sizeof(double),
+                                   (size_t)B, cudaMemcpyDeviceToDevice, st));
+    }
+    if (j.fwd_only) return CMD_OK;
+    cmd::ParamDerivs<NAT, Z, kAdjParams> pd;
+    std::memset(&pd, 0, sizeof(pd));
+    for (int q = 0; q < kAdjParams; ++q)
+        for (int at = 0; at < NAT; ++at) {
+            for (int sl = 0; sl < Z; ++sl)
+                std::memcpy(pd.DJ[q][at][sl], &DJ[(((size_t)q * NAT + at) * Z + sl) * 9], 9 * sizeof(double));
+            std::memcpy(pd.DB[q][at], &DB[((size_t)q * NAT + at) * 3], 3 * sizeof(double));
+            std::memcpy(pd.DA[q][at], &DA[((size_t)q * NAT + at) * 9], 9 * sizeof(double));
+        }
+    pd.has_DA = has_DA;
+    cmd::StreamVjpArgs v{};
+    v.G = G;
+    v.tiles = tiles;
+    v.nbr = a.nbr;
+    v.dt = j.dt;
+    v.n_steps = S;
+    v.drive = a.drive;
+    v.target = j.target;
+    v.mloc = j.mloc;
+    v.n_sites = a.n_sites;
+    v.gpart = h->sgpart.as<double>();
+    cmd::StreamArgs ar = a;              // recompute: no observables, no checkpoints
+    ar.ckpt = nullptr;
+    CUDA_TRY(cudaMemsetAsync(v.gpart, 0, (size_t)B * tiles * cmd::kPart * sizeof(double), st));
+    cmd::SVec lam{base, V}, lam2{base + B * V, V};
+    const cmd::SVec acc{base + 2 * B * V, V}, Sa{base + 3 * B * V, V}, Sb{base + 4 * B * V, V};
+    cmd::stream_lam_init_kernel<NAT><<<gridc, 256, 0, st>>>(v, lam);
+    double* seg = h->aseg.as<double>();
+    auto slot = [&](int64_t jj, int q) { return cmd::SVec{seg + (jj * 4 + q) * V, C * 4 * V}; };
+    const double dt = j.dt;
+    for (int64_t sg = K - 1; sg >= 0; --sg) {
+        const int64_t n0 = sg * C, n1 = std::min(n0 + C, S);
+        CUDA_TRY(cudaMemcpy2DAsync(seg, (size_t)C * 4 * V * sizeof(double), h->ackpt.as<double>() + sg * V,
+                                   (size_t)K * V * sizeof(double), (size_t)V * sizeof(double), (size_t)B,
+                                   cudaMemcpyDeviceToDevice, st));
+        for (int64_t n = n0; n < n1; ++n) {
+            const int64_t jj = n - n0;
+            const cmd::SVec y = slot(jj, 0);
+            const cmd::SVec last = n + 1 < n1 ? slot(jj + 1, 0) : none;
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, ar, 0, n, y, y, acc,
+                                                                                   slot(jj, 1), 0);
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, ar, 1, n, slot(jj, 1), y, acc,
+                                                                                   slot(jj, 2), 0);
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, ar, 2, n, slot(jj, 2), y, acc,
+                                                                                   slot(jj, 3), 0);
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, ar, 3, n, slot(jj, 3), y, acc,
+                                                                                   last, 0);
+        }
+        for (int64_t n = n1 - 1; n >= n0; --n) {
+            const int64_t jj = n - n0;
+            auto vjp = cmd::stream_vjp_kernel<NAT, Z, LZ, kAdjParams>;
+            vjp<<<grid, cmd::kStreamTile, 0, st>>>(cp, pd, v, 3, n, slot(jj, 3), lam, none, dt / 6.0, 0.0, Sa, acc,
+                                                   none, 0);
+            vjp<<<grid, cmd::kStreamTile, 0, st>>>(cp, pd, v, 2, n, slot(jj, 2), lam, Sa, dt / 3.0, dt, Sb, acc,
+                                                   none, 1);
+            vjp<<<grid, cmd::kStreamTile, 0, st>>>(cp, pd, v, 1, n, slot(jj, 1), lam, Sb, dt / 3.0, 0.5 * dt, Sa, acc,
+                                                   none, 1);
+            vjp<<<grid, cmd::kStreamTile, 0, st>>>(cp, pd, v, 0, n, slot(jj, 0), lam, Sa, dt / 6.0, 0.5 * dt, none,
+                                                   acc, lam2, 2);
+            std::swap(lam, lam2);
+        }
+        CUDA_TRY(cudaGetLastError());
+    }
+    cmd::stream_grad_kernel<<<(unsigned)B, 32, 0, st>>>(v.gpart, tiles, kAdjParams, j.out + 1, 1 + kAdjParams);
     CUDA_TRY(cudaGetLastError());
     return CMD_OK;
 }
@@ -1310,8 +1583,18 @@ int cmd_adjoint_rk4(cmd_handle* h, const cmd_adjoint_desc* d) {
     a.width = h->width;
     a.freq = h->freq;
     a.forward_only = fwd_only;
-    int rc = ty == 0 ? launch_adjoint<2, 3, 1>(h, a, DJ, DB, DA, has_DA, B)
+    // one CTA per trajectory when the batch fills the GPU, else streamed stages
+    const int tiles = (int)((h->lay.G + cmd::kStreamTile - 1) / cmd::kStreamTile);
+    const bool streamed = B < 148 && tiles >= 2 && B <= 65535;
+    int rc = CMD_OK;
+    if (streamed) {
+        StreamAdjJob j{B, S, C, K, fwd_only, din, dtgt, dtimes, h->amloc.as<double>(), dout, d->dt};
+        rc = ty == 0 ? stream_adjoint<2, 3, 1>(h, j, DJ, DB, DA, has_DA)
+                     : stream_adjoint<4, 6, 3>(h, j, DJ, DB, DA, has_DA);
+    } else {
+        rc = ty == 0 ? launch_adjoint<2, 3, 1>(h, a, DJ, DB, DA, has_DA, B)
                      : launch_adjoint<4, 6, 3>(h, a, DJ, DB, DA, has_DA, B);
+    }
     if (rc != CMD_OK) return rc;
     std::vector<double> out((size_t)B * (1 + kAdjParams));
     CUDA_TRY(cudaMemcpyAsync(out.data(), dout, out.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));

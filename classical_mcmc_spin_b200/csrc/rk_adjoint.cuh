@@ -77,96 +77,115 @@ struct AdjArgs {
     int forward_only;
 };
 
-// One fused RK4 stage s (0..3) over own cells, reading the stage input Yin at
-// the neighbours: k = H(Yin, ts) x Yin; H -> Hout when given;
+// One fused RK4 stage s (0..3) for cell g, reading the stage input Yin at
+// the neighbours: k = H(Yin) x Yin with the drive factors f1, f2 of the stage
+// time; H -> Hout when given;
 //   s = 0: acc = k,        Ynext = y + dt/2 k
 //   s = 1: acc = acc + 2k, Ynext = y + dt/2 k
 //   s = 2: acc = acc + 2k, Ynext = y + dt k
 //   s = 3:                 Ynext = y + dt/6 (acc + k)   (Ynext may alias y)
 // which is the RK4 step y + dt/6 (k1 + 2 k2 + 2 k3 + k4) of the reference GPU
-// stepper (integrator.cuh:115-139) summed in the same order.  Only own-cell
-// entries are written, so one barrier after the pass separates the stages.
-// When m is given, the own-cell sum of Yin is added to it.
+// stepper (integrator.cuh:115-139) summed in the same order.  Only the cell's
+// own entries are written.  Observables of Yin added to obs: OBS = 1: the sum
+// of the cell's spins over all atoms, obs[0..2]; OBS = 2: per atom class,
+// obs[3*atom + c], and twice the energy, sum_i S_i.(H_i - B_i) (static field,
+// before the drive; finish_rows_kernel applies the 1/2), in obs[3*NAT].
+template <int NAT, int Z, int LZ, int OBS>
+__device__ __forceinline__ void rk4_stage_cell(const Couplings<NAT, Z>& cp, const int* __restrict__ nbr, int G,
+                                               int g, double dt, int s, const double* __restrict__ Yin,
+                                               const double* y, double* acc, double* Ynext, double* __restrict__ Hout,
+                                               double f1, double f2, bool drive, double* obs) {
+    constexpr int NL = Z - LZ;
+    const double cy = s == 2 ? dt : 0.5 * dt;
+    double S[NAT][3];
+#pragma unroll
+    for (int at = 0; at < NAT; ++at)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) S[at][c] = Yin[(at * 3 + c) * G + g];
+    if (OBS > 0) {
+#pragma unroll
+        for (int at = 0; at < NAT; ++at)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) obs[(OBS == 2 ? 3 * at : 0) + c] += S[at][c];
+    }
+#pragma unroll
+    for (int at = 0; at < NAT; ++at) {
+        double H[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) H[d] = cp.has_field ? -cp.field[at][d] : 0.0;
+        if (cp.has_onsite) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                H[d] += 2.0 * cp.onsite[at][3 * d + 0] * S[at][0];
+                H[d] += 2.0 * cp.onsite[at][3 * d + 1] * S[at][1];
+                H[d] += 2.0 * cp.onsite[at][3 * d + 2] * S[at][2];
+            }
+        }
+#pragma unroll
+        for (int n = 0; n < LZ; ++n) {
+            const int pb = (at + 1 + n) % NAT;
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                H[d] += cp.J[at][n][3 * d] * S[pb][0] + cp.J[at][n][3 * d + 1] * S[pb][1] +
+                        cp.J[at][n][3 * d + 2] * S[pb][2];
+        }
+#pragma unroll
+        for (int mm = 0; mm < NL; ++mm) {
+            const int n = LZ + mm;
+            if (n < cp.zc[at]) {
+                const int p = nbr[((long long)g * NAT + at) * NL + mm];
+                const double P0 = Yin[p], P1 = Yin[p + G], P2 = Yin[p + 2 * G];
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    H[d] += cp.J[at][n][3 * d] * P0 + cp.J[at][n][3 * d + 1] * P1 + cp.J[at][n][3 * d + 2] * P2;
+            }
+        }
+        if (OBS == 2) {          // twice the energy: S.(H_static - B), before the drive enters
+#pragma unroll
+            for (int d = 0; d < 3; ++d) obs[3 * NAT] += S[at][d] * (H[d] - (cp.has_field ? cp.field[at][d] : 0.0));
+        }
+        if (drive) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) H[d] -= cp.d1[at][d] * f1 + cp.d2[at][d] * f2;
+        }
+        if (Hout) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) Hout[(at * 3 + d) * G + g] = H[d];
+        }
+        const double k[3] = {H[1] * S[at][2] - H[2] * S[at][1], H[2] * S[at][0] - H[0] * S[at][2],
+                             H[0] * S[at][1] - H[1] * S[at][0]};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const long long i = (long long)(at * 3 + c) * G + g;
+            const double yi = y[i];
+            if (s == 0) {
+                acc[i] = k[c];
+                Ynext[i] = 1.0 * yi + cy * k[c];
+            } else if (s < 3) {
+                acc[i] = acc[i] + 2.0 * k[c];
+                Ynext[i] = 1.0 * yi + cy * k[c];
+            } else if (Ynext) {
+                Ynext[i] = yi + (dt / 6.0) * (acc[i] + k[c]);
+            }
+        }
+    }
+}
+
+// rk4_stage_cell over this CTA's share of the cells (one CTA per trajectory);
+// when m is given, the own-cell sum of Yin over all atoms is added to m[0..2].
 template <int NAT, int Z, int LZ>
 __device__ __forceinline__ void rk4_stage(const Couplings<NAT, Z>& cp, const AdjArgs& a, int s,
                                           const double* __restrict__ Yin, const double* y, double* acc,
                                           double* Ynext, double* __restrict__ Hout, double ts, double* m) {
-    constexpr int NL = Z - LZ;
-    const int G = a.G, tid = threadIdx.x, nt = blockDim.x;
-    const double dt = a.dt;
     const bool drive = a.pulse.a1 != 0.0 || a.pulse.a2 != 0.0;
     const double f1 = drive ? drive_factor(a.pulse.a1, ts - a.pulse.t1, a.width, a.freq) : 0.0;
     const double f2 = drive ? drive_factor(a.pulse.a2, ts - a.pulse.t2, a.width, a.freq) : 0.0;
-    const double cy = s == 2 ? dt : 0.5 * dt;
-    for (int g = tid; g < G; g += nt) {
-        double S[NAT][3];
-#pragma unroll
-        for (int at = 0; at < NAT; ++at)
-#pragma unroll
-            for (int c = 0; c < 3; ++c) S[at][c] = Yin[(at * 3 + c) * G + g];
-        if (m) {
-#pragma unroll
-            for (int at = 0; at < NAT; ++at)
-#pragma unroll
-                for (int c = 0; c < 3; ++c) m[c] += S[at][c];
-        }
-#pragma unroll
-        for (int at = 0; at < NAT; ++at) {
-            double H[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) H[d] = cp.has_field ? -cp.field[at][d] : 0.0;
-            if (cp.has_onsite) {
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    H[d] += 2.0 * cp.onsite[at][3 * d + 0] * S[at][0];
-                    H[d] += 2.0 * cp.onsite[at][3 * d + 1] * S[at][1];
-                    H[d] += 2.0 * cp.onsite[at][3 * d + 2] * S[at][2];
-                }
-            }
-#pragma unroll
-            for (int n = 0; n < LZ; ++n) {
-                const int pb = (at + 1 + n) % NAT;
-#pragma unroll
-                for (int d = 0; d < 3; ++d)
-                    H[d] += cp.J[at][n][3 * d] * S[pb][0] + cp.J[at][n][3 * d + 1] * S[pb][1] +
-                            cp.J[at][n][3 * d + 2] * S[pb][2];
-            }
-#pragma unroll
-            for (int mm = 0; mm < NL; ++mm) {
-                const int n = LZ + mm;
-                if (n < cp.zc[at]) {
-                    const int p = a.nbr[((long long)g * NAT + at) * NL + mm];
-                    const double P0 = Yin[p], P1 = Yin[p + G], P2 = Yin[p + 2 * G];
-#pragma unroll
-                    for (int d = 0; d < 3; ++d)
-                        H[d] += cp.J[at][n][3 * d] * P0 + cp.J[at][n][3 * d + 1] * P1 + cp.J[at][n][3 * d + 2] * P2;
-                }
-            }
-            if (drive) {
-#pragma unroll
-                for (int d = 0; d < 3; ++d) H[d] -= cp.d1[at][d] * f1 + cp.d2[at][d] * f2;
-            }
-            if (Hout) {
-#pragma unroll
-                for (int d = 0; d < 3; ++d) Hout[(at * 3 + d) * G + g] = H[d];
-            }
-            const double k[3] = {H[1] * S[at][2] - H[2] * S[at][1], H[2] * S[at][0] - H[0] * S[at][2],
-                                 H[0] * S[at][1] - H[1] * S[at][0]};
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const long long i = (long long)(at * 3 + c) * G + g;
-                const double yi = y[i];
-                if (s == 0) {
-                    acc[i] = k[c];
-                    Ynext[i] = 1.0 * yi + cy * k[c];
-                } else if (s < 3) {
-                    acc[i] = acc[i] + 2.0 * k[c];
-                    Ynext[i] = 1.0 * yi + cy * k[c];
-                } else if (Ynext) {
-                    Ynext[i] = yi + (dt / 6.0) * (acc[i] + k[c]);
-                }
-            }
-        }
+    for (int g = threadIdx.x; g < a.G; g += blockDim.x) {
+        if (m)
+            rk4_stage_cell<NAT, Z, LZ, 1>(cp, a.nbr, a.G, g, a.dt, s, Yin, y, acc, Ynext, Hout, f1, f2, drive, m);
+        else
+            rk4_stage_cell<NAT, Z, LZ, 0>(cp, a.nbr, a.G, g, a.dt, s, Yin, y, acc, Ynext, Hout, f1, f2, drive,
+                                          nullptr);
     }
 }
 
@@ -231,8 +250,9 @@ adjoint_forward_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __gri
     if (tid == 0) T.loss[0] = loss;
 }
 
-// One stage VJP over own cells at stage input Y (time ts) with cotangent
-// v = ca lam + cb Sprev (Sprev unused when cb == 0):
+// One stage VJP for cell g at stage input Y with cotangent
+// v = ca lam + cb Sprev (Sprev unused when cb == 0) and the drive factors
+// f1, f2 of the stage time:
 //   H_i  = field at Y (static + drive),   Hbar_i = S_i x v_i
 //   Yb_i = v_i x H_i + 2 A_i^T Hbar_i + sum_n J_n Hbar_partner(n)
 //   thetabar_q += Hbar_i . (2 DA_q S_i - DB_q) + S_i . sum_n DJ_q,n Hbar_partner(n)
@@ -241,17 +261,13 @@ adjoint_forward_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __gri
 // step, per component).  lam, Sprev and Y are read at the partners, so
 // lam_out and Sout must be other buffers.
 template <int NAT, int Z, int LZ, int NQ>
-__device__ __forceinline__ void stage_vjp(const Couplings<NAT, Z>& cp, const ParamDerivs<NAT, Z, NQ>& pd,
-                                          const AdjArgs& a, const double* __restrict__ Y,
-                                          const double* __restrict__ lam, const double* __restrict__ Sprev,
-                                          double ca, double cb, double ts, double* __restrict__ Sout,
-                                          double* __restrict__ acc, double* __restrict__ lam_out, int mode,
-                                          const double* dl, double (&gq)[NQ]) {
+__device__ __forceinline__ void vjp_cell(const Couplings<NAT, Z>& cp, const ParamDerivs<NAT, Z, NQ>& pd,
+                                         const int* __restrict__ nbr, int G, int g, const double* __restrict__ Y,
+                                         const double* __restrict__ lam, const double* __restrict__ Sprev, double ca,
+                                         double cb, double f1, double f2, bool drive, double* __restrict__ Sout,
+                                         double* __restrict__ acc, double* __restrict__ lam_out, int mode,
+                                         const double* dl, double (&gq)[NQ]) {
     constexpr int NL = Z - LZ;
-    const int G = a.G, tid = threadIdx.x, nt = blockDim.x;
-    const bool drive = a.pulse.a1 != 0.0 || a.pulse.a2 != 0.0;
-    const double f1 = drive ? drive_factor(a.pulse.a1, ts - a.pulse.t1, a.width, a.freq) : 0.0;
-    const double f2 = drive ? drive_factor(a.pulse.a2, ts - a.pulse.t2, a.width, a.freq) : 0.0;
     auto cot = [&](long long i0, double (&v)[3]) {
         v[0] = ca * lam[i0];
         v[1] = ca * lam[i0 + G];
@@ -273,92 +289,107 @@ __device__ __forceinline__ void stage_vjp(const Couplings<NAT, Z>& cp, const Par
         Q[1] = P[2] * v[0] - P[0] * v[2];
         Q[2] = P[0] * v[1] - P[1] * v[0];
     };
-    for (int g = tid; g < G; g += nt) {
 #pragma unroll 1
-        for (int at = 0; at < NAT; ++at) {
-            const long long i0 = (long long)(at * 3) * G + g;
-            double Sown[3], hown[3];
-            partner(i0, Sown, hown);
-            const double S0 = Sown[0], S1 = Sown[1], S2 = Sown[2];
-            double H[3], sb[3] = {0.0, 0.0, 0.0};
+    for (int at = 0; at < NAT; ++at) {
+        const long long i0 = (long long)(at * 3) * G + g;
+        double Sown[3], hown[3];
+        partner(i0, Sown, hown);
+        const double S0 = Sown[0], S1 = Sown[1], S2 = Sown[2];
+        double H[3], sb[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-            for (int d = 0; d < 3; ++d) H[d] = cp.has_field ? -cp.field[at][d] : 0.0;
-            if (cp.has_onsite) {
+        for (int d = 0; d < 3; ++d) H[d] = cp.has_field ? -cp.field[at][d] : 0.0;
+        if (cp.has_onsite) {
 #pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    H[d] += 2.0 * cp.onsite[at][3 * d + 0] * S0;
-                    H[d] += 2.0 * cp.onsite[at][3 * d + 1] * S1;
-                    H[d] += 2.0 * cp.onsite[at][3 * d + 2] * S2;
-                    sb[d] += 2.0 * (cp.onsite[at][d] * hown[0] + cp.onsite[at][3 + d] * hown[1] +
-                                    cp.onsite[at][6 + d] * hown[2]);
-                }
+            for (int d = 0; d < 3; ++d) {
+                H[d] += 2.0 * cp.onsite[at][3 * d + 0] * S0;
+                H[d] += 2.0 * cp.onsite[at][3 * d + 1] * S1;
+                H[d] += 2.0 * cp.onsite[at][3 * d + 2] * S2;
+                sb[d] += 2.0 * (cp.onsite[at][d] * hown[0] + cp.onsite[at][3 + d] * hown[1] +
+                                cp.onsite[at][6 + d] * hown[2]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            double t = -(hown[0] * pd.DB[q][at][0] + hown[1] * pd.DB[q][at][1] + hown[2] * pd.DB[q][at][2]);
+            if (pd.has_DA) {
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    t += 2.0 * hown[d] * (pd.DA[q][at][3 * d] * S0 + pd.DA[q][at][3 * d + 1] * S1 +
+                                          pd.DA[q][at][3 * d + 2] * S2);
+            }
+            gq[q] += t;
+        }
+        // bond n with partner spin P and partner Hbar Q
+        auto bond = [&](int n, const double (&P)[3], const double (&Q)[3]) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                H[d] += cp.J[at][n][3 * d] * P[0] + cp.J[at][n][3 * d + 1] * P[1] + cp.J[at][n][3 * d + 2] * P[2];
+                sb[d] += cp.J[at][n][3 * d] * Q[0] + cp.J[at][n][3 * d + 1] * Q[1] + cp.J[at][n][3 * d + 2] * Q[2];
             }
 #pragma unroll
             for (int q = 0; q < NQ; ++q) {
-                double t = -(hown[0] * pd.DB[q][at][0] + hown[1] * pd.DB[q][at][1] + hown[2] * pd.DB[q][at][2]);
-                if (pd.has_DA) {
-#pragma unroll
-                    for (int d = 0; d < 3; ++d)
-                        t += 2.0 * hown[d] * (pd.DA[q][at][3 * d] * S0 + pd.DA[q][at][3 * d + 1] * S1 +
-                                              pd.DA[q][at][3 * d + 2] * S2);
-                }
-                gq[q] += t;
+                const double* D = pd.DJ[q][at][n];
+                gq[q] += S0 * (D[0] * Q[0] + D[1] * Q[1] + D[2] * Q[2]) +
+                         S1 * (D[3] * Q[0] + D[4] * Q[1] + D[5] * Q[2]) +
+                         S2 * (D[6] * Q[0] + D[7] * Q[1] + D[8] * Q[2]);
             }
-            // bond n with partner spin P and partner Hbar Q
-            auto bond = [&](int n, const double (&P)[3], const double (&Q)[3]) {
+        };
 #pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    H[d] += cp.J[at][n][3 * d] * P[0] + cp.J[at][n][3 * d + 1] * P[1] + cp.J[at][n][3 * d + 2] * P[2];
-                    sb[d] += cp.J[at][n][3 * d] * Q[0] + cp.J[at][n][3 * d + 1] * Q[1] + cp.J[at][n][3 * d + 2] * Q[2];
-                }
+        for (int n = 0; n < LZ; ++n) {
+            const int pb = (at + 1 + n) % NAT;
+            double P[3], Q[3];
+            partner((long long)(pb * 3) * G + g, P, Q);
+            bond(n, P, Q);
+        }
 #pragma unroll
-                for (int q = 0; q < NQ; ++q) {
-                    const double* D = pd.DJ[q][at][n];
-                    gq[q] += S0 * (D[0] * Q[0] + D[1] * Q[1] + D[2] * Q[2]) +
-                             S1 * (D[3] * Q[0] + D[4] * Q[1] + D[5] * Q[2]) +
-                             S2 * (D[6] * Q[0] + D[7] * Q[1] + D[8] * Q[2]);
-                }
-            };
-#pragma unroll
-            for (int n = 0; n < LZ; ++n) {
-                const int pb = (at + 1 + n) % NAT;
+        for (int m = 0; m < NL; ++m) {
+            const int n = LZ + m;
+            if (n < cp.zc[at]) {
                 double P[3], Q[3];
-                partner((long long)(pb * 3) * G + g, P, Q);
+                partner(nbr[((long long)g * NAT + at) * NL + m], P, Q);
                 bond(n, P, Q);
             }
+        }
+        if (drive) {
 #pragma unroll
-            for (int m = 0; m < NL; ++m) {
-                const int n = LZ + m;
-                if (n < cp.zc[at]) {
-                    double P[3], Q[3];
-                    partner(a.nbr[((long long)g * NAT + at) * NL + m], P, Q);
-                    bond(n, P, Q);
-                }
-            }
-            if (drive) {
+            for (int d = 0; d < 3; ++d) H[d] -= cp.d1[at][d] * f1 + cp.d2[at][d] * f2;
+        }
+        double v[3];
+        cot(i0, v);
+        sb[0] += v[1] * H[2] - v[2] * H[1];
+        sb[1] += v[2] * H[0] - v[0] * H[2];
+        sb[2] += v[0] * H[1] - v[1] * H[0];
 #pragma unroll
-                for (int d = 0; d < 3; ++d) H[d] -= cp.d1[at][d] * f1 + cp.d2[at][d] * f2;
-            }
-            double v[3];
-            cot(i0, v);
-            sb[0] += v[1] * H[2] - v[2] * H[1];
-            sb[1] += v[2] * H[0] - v[0] * H[2];
-            sb[2] += v[0] * H[1] - v[1] * H[0];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                const long long i = i0 + d * G;
-                if (mode == 0) {
-                    Sout[i] = sb[d];
-                    acc[i] = lam[i] + sb[d];
-                } else if (mode == 1) {
-                    Sout[i] = sb[d];
-                    acc[i] = acc[i] + sb[d];
-                } else {
-                    lam_out[i] = acc[i] + sb[d] + dl[d];
-                }
+        for (int d = 0; d < 3; ++d) {
+            const long long i = i0 + d * G;
+            if (mode == 0) {
+                Sout[i] = sb[d];
+                acc[i] = lam[i] + sb[d];
+            } else if (mode == 1) {
+                Sout[i] = sb[d];
+                acc[i] = acc[i] + sb[d];
+            } else {
+                lam_out[i] = acc[i] + sb[d] + dl[d];
             }
         }
     }
+}
+
+// vjp_cell over this CTA's share of the cells (one CTA per trajectory) at the
+// stage time ts.
+template <int NAT, int Z, int LZ, int NQ>
+__device__ __forceinline__ void stage_vjp(const Couplings<NAT, Z>& cp, const ParamDerivs<NAT, Z, NQ>& pd,
+                                          const AdjArgs& a, const double* __restrict__ Y,
+                                          const double* __restrict__ lam, const double* __restrict__ Sprev,
+                                          double ca, double cb, double ts, double* __restrict__ Sout,
+                                          double* __restrict__ acc, double* __restrict__ lam_out, int mode,
+                                          const double* dl, double (&gq)[NQ]) {
+    const bool drive = a.pulse.a1 != 0.0 || a.pulse.a2 != 0.0;
+    const double f1 = drive ? drive_factor(a.pulse.a1, ts - a.pulse.t1, a.width, a.freq) : 0.0;
+    const double f2 = drive ? drive_factor(a.pulse.a2, ts - a.pulse.t2, a.width, a.freq) : 0.0;
+    for (int g = threadIdx.x; g < a.G; g += blockDim.x)
+        vjp_cell<NAT, Z, LZ, NQ>(cp, pd, a.nbr, a.G, g, Y, lam, Sprev, ca, cb, f1, f2, drive, Sout, acc, lam_out,
+                                 mode, dl, gq);
 }
 
 template <int NAT, int Z, int LZ, int NQ>

@@ -94,8 +94,8 @@ def test_dopri5_fixed_matches_reference_gpu(api, oracle):
         assert np.abs(obs[r, :9] - o.magnetizations(rs[r])).max() <= 1e-13
 
 
-def test_global_rk4_fallback_for_large_lattice(api, oracle):
-    """48x48 honeycomb (4608 spins) does not fit the resident kernel: RK4 runs in global memory."""
+def test_streamed_rk4_for_large_lattice(api, oracle):
+    """48x48 honeycomb (4608 spins) does not fit the resident kernel: RK4 runs as streamed stage kernels."""
     lat, o = _kitaev(oracle, 48, 48)
     s0 = _spins(lat.lattice_size, 34)
     h = lat.to_gpu()
