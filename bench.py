@@ -158,6 +158,143 @@ def profile_traffic():
     return None
 
 
+# --------------------------------------------------------------------------- further workloads
+R111 = np.ones(3) / np.sqrt(3.0)
+STREAM_BYTES_PER_SPIN_STEP = 408.0   # stages 72 + 120 + 120 + 96 B (input, y, RK4 sum, next input)
+
+
+def leg_uneven(torch, dev, max_steps=10000, T1=100.0, B=512):
+    """Uneven batch: 512 trajectories, honeycomb L in {8..32} and pyrochlore 16L^3, L in {4, 6, 8}, drawn from
+    seed 3; controlled RK45 at tol 1e-10, T_end = 100, cap 1e4 accepted steps; one persistent launch."""
+    from classical_mcmc_spin_b200 import gpu_api
+    from classical_mcmc_spin_b200.lattice import Lattice
+    from classical_mcmc_spin_b200.states import random_unit_spins
+    opts = [("honeycomb", L) for L in (8, 12, 16, 24, 32)] + [("pyrochlore", L) for L in (4, 6, 8)]
+    pick = np.random.default_rng(3).integers(0, len(opts), size=B)
+    handles = {}
+    for k in sorted(set(pick.tolist())):
+        kind, L = opts[k]
+        lat = (Lattice.kitaev(L, L, 1) if kind == "honeycomb" else
+               Lattice.pyrochlore_non_kramer(L, L, L, cubic=True, Jzz=1.0, Jpm=0.05, Jpmpm=0.02))
+        handles[k] = (lat, lat.to_gpu())
+    specs = []
+    for b in range(B):
+        lat, h = handles[int(pick[b])]
+        specs.append(dict(handle=h, state=random_unit_spins(lat.lattice_size, 3000 + b).ravel(), T0=0.0, T1=T1,
+                          dt=0.01, max_rows=max_steps + 2))
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    out = gpu_api.run_uneven(specs, "rk45", 1e-10, 1e-10, max_steps=max_steps)
+    torch.cuda.synchronize(dev)
+    wall = time.perf_counter() - t0
+    acc = sum(o[2][1] for o in out)
+    rej = sum(o[2][2] for o in out)
+    work = sum(specs[b]["handle"].N * out[b][2][1] for b in range(B))
+    for _, h in handles.values():
+        h.close()
+    return {"value": work / wall, "unit": "accepted spin·RK45-steps/s", "wall_s": wall, "trajectories": B,
+            "accepted_steps": acc, "rejected_steps": rej, "spin_steps": work, "tol": 1e-10, "T_end": T1,
+            "types": {f"{opts[k][0]}_L{opts[k][1]}": int((pick == k).sum()) for k in handles},
+            "timing": "wall clock around the public call (host buffers in and out)"}
+
+
+def _adjoint_leg(torch, dev, build, theta, theta_target, n_params, B, S, dt, seed, ckpt):
+    from classical_mcmc_spin_b200 import adjoint as A
+    from classical_mcmc_spin_b200.states import random_unit_spins
+    lat = build(theta)
+    N = lat.lattice_size
+    h, ht = lat.to_gpu(), build(theta_target).to_gpu()
+    states = np.stack([random_unit_spins(N, seed * 1000 + b).ravel() for b in range(B)])
+    _, _, target = A.adjoint_rk4(ht, [], states, 0.0, dt, S, np.zeros((B, S + 1, 3)), forward_only=True)
+    dps = A.basis_lattices(build, n_params)
+    A.adjoint_rk4(h, dps, states[:1], 0.0, dt, 4, target[:1, :5], checkpoint_every=2)      # warm
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    loss_f, _, _ = A.adjoint_rk4(h, [], states, 0.0, dt, S, target, forward_only=True)
+    torch.cuda.synchronize(dev)
+    tf = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    loss, grad, _ = A.adjoint_rk4(h, dps, states, 0.0, dt, S, target, checkpoint_every=ckpt)
+    torch.cuda.synchronize(dev)
+    ta = time.perf_counter() - t0
+    h.close()
+    ht.close()
+    return {"spins": N, "trajectories": B, "rk4_steps": S, "dt": dt, "checkpoint_every": ckpt,
+            "forward_s": tf, "forward_plus_adjoint_s": ta, "ratio": ta / tf,
+            "forward_value": B * N * S / tf, "unit": UNIT, "loss_mean": float(np.mean(loss)),
+            "loss_forward_only_equal": bool(np.array_equal(loss, loss_f)),
+            "grad_mean": np.mean(grad, axis=0).tolist(),
+            "timing": "wall clock around the public call (host buffers in and out)"}
+
+
+def leg_adjoint_kitaev(torch, dev, S=20000):
+    """Adjoint: honeycomb 48x48 (4608 spins), 64 states (seed 4), RK4 dt 0.01, M_local loss against targets at
+    (K, G, G', J, h) = (-1, 0.3, -0.03, 0, 0.1); gradient at (-1, 0.25, -0.02, 0, 0) w.r.t. all five,
+    checkpoint every 141 steps."""
+    from classical_mcmc_spin_b200 import adjoint as A
+    build = lambda th: A.kitaev_lattice(th, 48, 48)
+    out = _adjoint_leg(torch, dev, build, np.array([-1.0, 0.25, -0.02, 0.0, 0.0]),
+                       np.array([-1.0, 0.3, -0.03, 0.0, 0.1]), 5, 64, S, 0.01, 4, 141)
+    out["workload"] = "adjoint_kitaev48x48_64traj_rk4"
+    return out
+
+
+def leg_pyrochlore(torch, dev, S=20000, S_adj=2000):
+    """Large pyrochlore: 16^3 conventional cells (65536 spins), Jzz=1, J+-=0.05, J+-+-=0.02, h=0.2 along [111],
+    32 states (seed 5), RK4 dt 0.005.  Forward through cmd_run_batch_device (device buffers, CUDA events, M and E
+    every step); adjoint w.r.t. (Jzz, J+-, J+-+-, h) against targets at (1, 0.06, 0.03, 0.25)."""
+    from classical_mcmc_spin_b200 import _native as nat
+    from classical_mcmc_spin_b200 import adjoint as A
+    from classical_mcmc_spin_b200.states import random_unit_spins
+    theta = np.array([1.0, 0.05, 0.02, 0.2])
+    build = lambda th: A.pyrochlore_lattice(th, 16, 16, 16, cubic=True)
+    lat = build(theta)
+    N, B, dt = lat.lattice_size, 32, 0.005
+    h = lat.to_gpu()
+    states = np.stack([random_unit_spins(N, 5000 + b).ravel() for b in range(B)])
+    d_states = torch.from_numpy(states).to(dev).contiguous()
+    rows = int(nat.lib().cmd_batch_rows(S, 1))
+    d_obs = torch.empty((B, rows, 10), dtype=torch.float64, device=dev)
+    d_fin = torch.empty_like(d_states)
+    desc = nat.BatchDesc()
+    desc.B = B
+    desc.states = d_states.data_ptr()
+    desc.shared_initial = 0
+    desc.method = nat.CMD_RK4
+    desc.width, desc.freq, desc.T0, desc.dt = 1.0, 0.0, 0.0, dt
+    desc.save_interval = 1
+    desc.obs = d_obs.data_ptr()
+    desc.final_states = d_fin.data_ptr()
+    launches = C.c_int32()
+    stream = torch.cuda.current_stream(dev)
+
+    def run(n):
+        desc.n_steps = n
+        nat.check(nat.lib().cmd_run_batch_device(h.ptr, C.byref(desc), C.c_void_p(stream.cuda_stream),
+                                                 C.byref(launches)), "cmd_run_batch_device")
+
+    run(8)                                   # warm
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    run(S)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1)
+    value = B * N * S / (ms * 1e-3)
+    norm_dev = float((d_fin.view(B, N, 3).norm(dim=2) - 1).abs().max().item())
+    fwd = {"value": value, "unit": UNIT, "ms": ms, "rk4_steps": S, "launches": launches.value,
+           "hbm_bytes_per_spin_step": STREAM_BYTES_PER_SPIN_STEP,
+           "achieved_gbs": STREAM_BYTES_PER_SPIN_STEP * value / 1e9,
+           "final_norm_dev_max": norm_dev, "observables_finite": bool(torch.isfinite(d_obs).all().item())}
+    del d_obs, d_fin, d_states
+    h.close()
+    adj = _adjoint_leg(torch, dev, build, theta, np.array([1.0, 0.06, 0.03, 0.25]), 4, B, S_adj, dt, 5,
+                       int(np.ceil(np.sqrt(S_adj))))
+    return {"workload": "pyrochlore16cubic_65536spins_32traj_rk4", "spins": N, "trajectories": B, "dt": dt,
+            "forward": fwd, "adjoint": adj}
+
+
 # --------------------------------------------------------------------------- CPU baseline
 def cpu_baseline(wl, target_s: float = 8.0):
     sys.path.insert(0, str(ROOT / "oracle"))
@@ -232,6 +369,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
     ap.add_argument("--no-peak", action="store_true", help="skip the DGEMM peak probe (profiling runs)")
+    ap.add_argument("--legs", default="uneven,adjoint,pyrochlore",
+                    help="further workloads to time on rank 0 (comma list; empty for none)")
+    ap.add_argument("--adjoint-steps", type=int, default=20000, help="RK4 steps of the 48x48 adjoint leg")
+    ap.add_argument("--pyro-steps", type=int, default=20000, help="RK4 steps of the 65536-spin forward leg")
+    ap.add_argument("--pyro-adjoint-steps", type=int, default=2000, help="RK4 steps of the 65536-spin adjoint")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -406,6 +548,15 @@ def main():
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu, _ = cpu_baseline(wl, target_s=args.cpu_seconds)
+    legs = {}
+    if rank == 0:
+        want = [x for x in args.legs.split(",") if x]
+        if "uneven" in want:
+            legs["uneven_rk45"] = leg_uneven(torch, dev)
+        if "adjoint" in want:
+            legs["adjoint_kitaev48"] = leg_adjoint_kitaev(torch, dev, S=args.adjoint_steps)
+        if "pyrochlore" in want:
+            legs["pyrochlore65536"] = leg_pyrochlore(torch, dev, S=args.pyro_steps, S_adj=args.pyro_adjoint_steps)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -418,7 +569,8 @@ def main():
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
                 "gpu_launches": n_launch, "plain_path": plain,
                 "batched_over_plain": (value / world) / plain["value"] if plain else None,
-                "adjoint_over_forward": None,
+                "adjoint_over_forward": legs["adjoint_kitaev48"]["ratio"] if "adjoint_kitaev48" in legs else None,
+                "legs": legs,
                 "checks": {"final_norm_dev_max": norm_dev, "observables_finite": finite}}
         print(json.dumps(line), flush=True)
     h.close()

@@ -503,7 +503,7 @@ int stream_forward(cmd_handle* h, const RunSpec& r, cudaStream_t st, int32_t* la
     constexpr int NR = 3 * NAT + 1;
     int32_t nl = 0;
     const int G = (int)h->lay.G;
-    const int tiles = (G + cmd::kStreamTile - 1) / cmd::kStreamTile;
+    const int tiles = (G + cmd::stream_cells<NAT>() - 1) / cmd::stream_cells<NAT>();
     const int64_t V = (int64_t)NAT * 3 * G;
     const int64_t B = r.B;
     if (B > 65535) return fail(CMD_ERR_UNSUPPORTED, "streamed batches are limited to 65535 trajectories");
@@ -1363,16 +1363,17 @@ struct StreamAdjJob {
     double dt;
 };
 
-template <int NAT, int Z, int LZ>
+template <int NAT, int Z, int LZ, int NQ>
 int stream_adjoint(cmd_handle* h, const StreamAdjJob& j, const std::vector<double>& DJ, const std::vector<double>& DB,
                    const std::vector<double>& DA, bool has_DA) {
     cudaStream_t st = h->stream;
     const int G = (int)h->lay.G;
-    const int tiles = (G + cmd::kStreamTile - 1) / cmd::kStreamTile;
+    const int tiles = (G + cmd::stream_cells<NAT>() - 1) / cmd::stream_cells<NAT>();
     const int64_t V = (int64_t)NAT * 3 * G, B = j.B, S = j.S, C = j.C, K = j.K;
     if (int rc = h->sbuf.ensure((size_t)5 * B * V * sizeof(double))) return rc;
     if (int rc = h->spart.ensure(((size_t)B * tiles * cmd::kPart + B) * sizeof(double))) return rc;
-    if (int rc = h->sgpart.ensure((size_t)B * tiles * cmd::kPart * sizeof(double))) return rc;
+    const int vtiles = (G + cmd::kStreamTile - 1) / cmd::kStreamTile;     // VJP: one cell per thread
+    if (int rc = h->sgpart.ensure((size_t)B * vtiles * cmd::kPart * sizeof(double))) return rc;
     double* base = h->sbuf.as<double>();
     double* d_loss = h->spart.as<double>() + (size_t)B * tiles * cmd::kPart;
     const bool driven = h->amp != 0.0;
@@ -1429,9 +1430,9 @@ int stream_adjoint(cmd_handle* h, const StreamAdjJob& j, const std::vector<doubl
                                    (size_t)B, cudaMemcpyDeviceToDevice, st));
     }
     if (j.fwd_only) return CMD_OK;
-    cmd::ParamDerivs<NAT, Z, kAdjParams> pd;
+    cmd::ParamDerivs<NAT, Z, NQ> pd;
     std::memset(&pd, 0, sizeof(pd));
-    for (int q = 0; q < kAdjParams; ++q)
+    for (int q = 0; q < NQ; ++q)
         for (int at = 0; at < NAT; ++at) {
             for (int sl = 0; sl < Z; ++sl)
                 std::memcpy(pd.DJ[q][at][sl], &DJ[(((size_t)q * NAT + at) * Z + sl) * 9], 9 * sizeof(double));
@@ -1441,7 +1442,7 @@ int stream_adjoint(cmd_handle* h, const StreamAdjJob& j, const std::vector<doubl
     pd.has_DA = has_DA;
     cmd::StreamVjpArgs v{};
     v.G = G;
-    v.tiles = tiles;
+    v.tiles = vtiles;
     v.nbr = a.nbr;
     v.dt = j.dt;
     v.n_steps = S;
@@ -1452,7 +1453,8 @@ int stream_adjoint(cmd_handle* h, const StreamAdjJob& j, const std::vector<doubl
     v.gpart = h->sgpart.as<double>();
     cmd::StreamArgs ar = a;              // recompute: no observables, no checkpoints
     ar.ckpt = nullptr;
-    CUDA_TRY(cudaMemsetAsync(v.gpart, 0, (size_t)B * tiles * cmd::kPart * sizeof(double), st));
+    CUDA_TRY(cudaMemsetAsync(v.gpart, 0, (size_t)B * vtiles * cmd::kPart * sizeof(double), st));
+    const dim3 vgrid(vtiles, (unsigned)B);
     cmd::SVec lam{base, V}, lam2{base + B * V, V};
     const cmd::SVec acc{base + 2 * B * V, V}, Sa{base + 3 * B * V, V}, Sb{base + 4 * B * V, V};
     cmd::stream_lam_init_kernel<NAT><<<gridc, 256, 0, st>>>(v, lam);
@@ -1479,20 +1481,20 @@ int stream_adjoint(cmd_handle* h, const StreamAdjJob& j, const std::vector<doubl
         }
         for (int64_t n = n1 - 1; n >= n0; --n) {
             const int64_t jj = n - n0;
-            auto vjp = cmd::stream_vjp_kernel<NAT, Z, LZ, kAdjParams>;
-            vjp<<<grid, cmd::kStreamTile, 0, st>>>(cp, pd, v, 3, n, slot(jj, 3), lam, none, dt / 6.0, 0.0, Sa, acc,
+            auto vjp = cmd::stream_vjp_kernel<NAT, Z, LZ, NQ>;
+            vjp<<<vgrid, cmd::kStreamTile, 0, st>>>(cp, pd, v, 3, n, slot(jj, 3), lam, none, dt / 6.0, 0.0, Sa, acc,
                                                    none, 0);
-            vjp<<<grid, cmd::kStreamTile, 0, st>>>(cp, pd, v, 2, n, slot(jj, 2), lam, Sa, dt / 3.0, dt, Sb, acc,
+            vjp<<<vgrid, cmd::kStreamTile, 0, st>>>(cp, pd, v, 2, n, slot(jj, 2), lam, Sa, dt / 3.0, dt, Sb, acc,
                                                    none, 1);
-            vjp<<<grid, cmd::kStreamTile, 0, st>>>(cp, pd, v, 1, n, slot(jj, 1), lam, Sb, dt / 3.0, 0.5 * dt, Sa, acc,
+            vjp<<<vgrid, cmd::kStreamTile, 0, st>>>(cp, pd, v, 1, n, slot(jj, 1), lam, Sb, dt / 3.0, 0.5 * dt, Sa, acc,
                                                    none, 1);
-            vjp<<<grid, cmd::kStreamTile, 0, st>>>(cp, pd, v, 0, n, slot(jj, 0), lam, Sa, dt / 6.0, 0.5 * dt, none,
+            vjp<<<vgrid, cmd::kStreamTile, 0, st>>>(cp, pd, v, 0, n, slot(jj, 0), lam, Sa, dt / 6.0, 0.5 * dt, none,
                                                    acc, lam2, 2);
             std::swap(lam, lam2);
         }
         CUDA_TRY(cudaGetLastError());
     }
-    cmd::stream_grad_kernel<<<(unsigned)B, 32, 0, st>>>(v.gpart, tiles, kAdjParams, j.out + 1, 1 + kAdjParams);
+    cmd::stream_grad_kernel<<<(unsigned)B, 32, 0, st>>>(v.gpart, vtiles, NQ, j.out + 1, 1 + kAdjParams);
     CUDA_TRY(cudaGetLastError());
     return CMD_OK;
 }
@@ -1584,13 +1586,19 @@ int cmd_adjoint_rk4(cmd_handle* h, const cmd_adjoint_desc* d) {
     a.freq = h->freq;
     a.forward_only = fwd_only;
     // one CTA per trajectory when the batch fills the GPU, else streamed stages
-    const int tiles = (int)((h->lay.G + cmd::kStreamTile - 1) / cmd::kStreamTile);
+    const int cpt = cmd::kStreamTile / std::max(1, h->NA);
+    const int tiles = (int)((h->lay.G + cpt - 1) / cpt);
     const bool streamed = B < 148 && tiles >= 2 && B <= 65535;
     int rc = CMD_OK;
     if (streamed) {
         StreamAdjJob j{B, S, C, K, fwd_only, din, dtgt, dtimes, h->amloc.as<double>(), dout, d->dt};
-        rc = ty == 0 ? stream_adjoint<2, 3, 1>(h, j, DJ, DB, DA, has_DA)
-                     : stream_adjoint<4, 6, 3>(h, j, DJ, DB, DA, has_DA);
+        // the VJP carries as many parameter cotangents as requested (4 or 5)
+        if (d->n_params <= 4)
+            rc = ty == 0 ? stream_adjoint<2, 3, 1, 4>(h, j, DJ, DB, DA, has_DA)
+                         : stream_adjoint<4, 6, 3, 4>(h, j, DJ, DB, DA, has_DA);
+        else
+            rc = ty == 0 ? stream_adjoint<2, 3, 1, 5>(h, j, DJ, DB, DA, has_DA)
+                         : stream_adjoint<4, 6, 3, 5>(h, j, DJ, DB, DA, has_DA);
     } else {
         rc = ty == 0 ? launch_adjoint<2, 3, 1>(h, a, DJ, DB, DA, has_DA, B)
                      : launch_adjoint<4, 6, 3>(h, a, DJ, DB, DA, has_DA, B);

@@ -259,7 +259,8 @@ adjoint_forward_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __gri
 // then per own entry  mode 0: Sout = Yb, acc = lam + Yb;  mode 1: Sout = Yb,
 // acc += Yb;  mode 2: lam_out = acc + Yb + dl (dl: the loss cotangent at this
 // step, per component).  lam, Sprev and Y are read at the partners, so
-// lam_out and Sout must be other buffers.
+// lam_out and Sout must be other buffers.  The atoms run in a rolled loop:
+// one copy of this large body keeps the instruction cache warm.
 template <int NAT, int Z, int LZ, int NQ>
 __device__ __forceinline__ void vjp_cell(const Couplings<NAT, Z>& cp, const ParamDerivs<NAT, Z, NQ>& pd,
                                          const int* __restrict__ nbr, int G, int g, const double* __restrict__ Y,

@@ -2,22 +2,24 @@
 // resident CTA (e.g. the 65536-spin conventional-cubic pyrochlore), with state
 // streamed through L2 / HBM.
 //
-// Every RK4 stage is ONE launch over a (cell tile, trajectory) grid: thread g
-// of tile t of trajectory b advances cell t*kStreamTile + g with
-// rk4_stage_cell, so all SMs work on every trajectory and the kernel boundary
-// is the only barrier between stages (no device-side waits anywhere).  The
-// adjoint uses the same launches for its segment recompute and one vjp_cell
-// launch per stage for the reverse sweep.
+// Every RK4 stage is ONE launch over a (cell tile, trajectory) grid; each
+// thread advances one site (cell, atom) with rk4_stage_site, the atom uniform
+// per warp, so all SMs work on every trajectory and the kernel boundary is the
+// only barrier between stages (no device-side waits anywhere).  The adjoint
+// uses the same launches for its segment recompute and one vjp_cell launch per
+// stage for the reverse sweep (one cell per thread).
 //
 // Vectors are cell-major SoA per trajectory, v[(atom*3 + c)*G + g], trajectory
 // b at p + b*stride (SVec).  Per stage a cell reads its stage input (own and
 // partners'), y and the RK4 sum, and writes the sum and the next stage input:
-// 120 B per spin-stage, 480 B per spin-step when nothing is cached.
+// per spin 72 B (stage 0: y in, sum and next input out), 120 B (stages 1, 2)
+// and 96 B (stage 3: y written in place), 408 B per spin-step when the
+// partners' reads hit in cache.
 //
 // Observables, in a fixed summation order without atomics: the stage-0 launch
 // of step n leaves one partial per (trajectory, tile) (spin sums per atom class
 // and the energy), and the first CTA of each trajectory in the stage-1 launch
-// of the same step sums them over the tiles in tile order.  That CTA writes the
+// of the same step sums them over the tiles in a fixed order.  That CTA writes the
 // raw row (as rk4_resident's rows: finished by finish_rows_kernel) and/or the
 // M_local loss terms.  The state after the last step is summed by
 // stream_obs_kernel + stream_reduce_kernel.
@@ -59,6 +61,110 @@ struct StreamArgs {
     long long ckpt_every, n_ckpt, V;
 };
 
+// Threads of a CTA: NAT groups of kStreamTile/NAT consecutive threads, group
+// a advancing atom a of the CTA's kStreamTile/NAT cells (the atom is uniform
+// per warp for NAT in {1, 2, 4, 8}).
+template <int NAT>
+constexpr int stream_cells() { return kStreamTile / NAT; }
+
+template <int V>
+struct AtomTag {
+    static constexpr int value = V;
+};
+
+// f(AtomTag<at>) with `at` (0 <= at < NAT) as a compile-time constant, so the
+// couplings of the atom stay constant-bank operands.
+template <int NAT, int AT = 0, class F>
+__device__ __forceinline__ void with_atom(int at, F&& f) {
+    if constexpr (AT < NAT) {
+        if (at == AT)
+            f(AtomTag<AT>{});
+        else
+            with_atom<NAT, AT + 1>(at, f);
+    }
+}
+
+template <int NAT>
+__device__ __forceinline__ void stream_site(int& at, int& g) {
+    constexpr int CPT = stream_cells<NAT>();
+    at = (int)threadIdx.x / CPT;
+    g = (int)blockIdx.x * CPT + ((int)threadIdx.x - at * CPT);
+}
+
+// rk4_stage_cell for site (cell g, atom AT) alone.  Every load comes before
+// the first store (acc / Ynext may alias y), so a thread's loads are all in
+// flight together.
+template <int NAT, int Z, int LZ, int AT, int OBS>
+__device__ __forceinline__ void rk4_stage_site(const Couplings<NAT, Z>& cp, const int* __restrict__ nbr, int G,
+                                               int g, double dt, int s, const double* __restrict__ Yin,
+                                               const double* y, double* acc, double* Ynext, double f1, double f2,
+                                               bool drive, double* obs) {
+    constexpr int NL = Z - LZ;
+    const long long i0 = (long long)(AT * 3) * G + g;
+    double S[3], yv[3], av[3], H[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) S[c] = Yin[i0 + c * G];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        yv[c] = s == 0 ? S[c] : y[i0 + c * G];
+        av[c] = (s == 0 || !acc) ? 0.0 : acc[i0 + c * G];
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) H[d] = cp.has_field ? -cp.field[AT][d] : 0.0;
+    if (cp.has_onsite) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            H[d] += 2.0 * cp.onsite[AT][3 * d + 0] * S[0];
+            H[d] += 2.0 * cp.onsite[AT][3 * d + 1] * S[1];
+            H[d] += 2.0 * cp.onsite[AT][3 * d + 2] * S[2];
+        }
+    }
+#pragma unroll
+    for (int n = 0; n < LZ; ++n) {
+        const long long ip = (long long)(((AT + 1 + n) % NAT) * 3) * G + g;
+        const double P0 = Yin[ip], P1 = Yin[ip + G], P2 = Yin[ip + 2 * G];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            H[d] += cp.J[AT][n][3 * d] * P0 + cp.J[AT][n][3 * d + 1] * P1 + cp.J[AT][n][3 * d + 2] * P2;
+    }
+#pragma unroll
+    for (int m = 0; m < NL; ++m) {
+        const int n = LZ + m;
+        if (n < cp.zc[AT]) {
+            const int p = nbr[((long long)g * NAT + AT) * NL + m];
+            const double P0 = Yin[p], P1 = Yin[p + G], P2 = Yin[p + 2 * G];
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                H[d] += cp.J[AT][n][3 * d] * P0 + cp.J[AT][n][3 * d + 1] * P1 + cp.J[AT][n][3 * d + 2] * P2;
+        }
+    }
+    if (OBS == 2) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) obs[3 * AT + c] += S[c];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) obs[3 * NAT] += S[d] * (H[d] - (cp.has_field ? cp.field[AT][d] : 0.0));
+    }
+    if (drive) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) H[d] -= cp.d1[AT][d] * f1 + cp.d2[AT][d] * f2;
+    }
+    const double k[3] = {H[1] * S[2] - H[2] * S[1], H[2] * S[0] - H[0] * S[2], H[0] * S[1] - H[1] * S[0]};
+    const double cy = s == 2 ? dt : 0.5 * dt;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const long long i = i0 + c * G;
+        if (s == 0) {
+            acc[i] = k[c];
+            Ynext[i] = 1.0 * yv[c] + cy * k[c];
+        } else if (s < 3) {
+            acc[i] = av[c] + 2.0 * k[c];
+            Ynext[i] = 1.0 * yv[c] + cy * k[c];
+        } else if (Ynext) {
+            Ynext[i] = yv[c] + (dt / 6.0) * (av[c] + k[c]);
+        }
+    }
+}
+
 // Envelope factors of trajectory b for stage s of step n.
 __device__ __forceinline__ void stream_drive(const StreamArgs& a, int b, long long n, int s, double& f1,
                                              double& f2) {
@@ -72,17 +178,21 @@ __device__ __forceinline__ void stream_drive(const StreamArgs& a, int b, long lo
     f2 = d[1];
 }
 
-// Sums the tile partials of step n of trajectory b (blockIdx.y) in tile order
-// and writes its raw row and / or loss terms.  Called by a whole CTA.
+// Sums the tile partials of step n of trajectory b and writes its raw row
+// and / or loss terms.  Called by a whole CTA: warp w sums values w, w+nwarps,
+// ...; lane l adds tiles l, l+32, ... in order, then a fixed butterfly adds
+// the lanes, so the order never depends on timing.
 template <int NAT>
 __device__ void stream_reduce(const StreamArgs& a, int b, long long n, double* sh) {
     constexpr int NR = 3 * NAT + 1;
-    const int tid = threadIdx.x;
-    if (tid < NR) {
-        const double* p = a.part + (long long)b * a.tiles * kPart + tid;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    const double* p = a.part + (long long)b * a.tiles * kPart;
+    for (int q = warp; q < NR; q += nw) {
         double s = 0.0;
-        for (int t = 0; t < a.tiles; ++t) s += p[(long long)t * kPart];
-        sh[tid] = s;
+        for (int t = lane; t < a.tiles; t += 32) s += p[(long long)t * kPart + q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) sh[q] = s;
     }
     __syncthreads();
     if (a.raw && tid < NR) {
@@ -125,14 +235,15 @@ __device__ __forceinline__ void stream_store_partial(const StreamArgs& a, int b,
 // the observables' partials of Yin (= y_n) and the checkpoint of y_n; the
 // first tile of stage 1 finishes step n's observables.
 template <int NAT, int Z, int LZ>
-__global__ void __launch_bounds__(kStreamTile, 2)
+__global__ void __launch_bounds__(kStreamTile, 4)
 stream_stage_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_constant__ StreamArgs a, int s,
                     long long n, SVec Yin, SVec y, SVec acc, SVec Ynext, int with_obs) {
     constexpr int NR = 3 * NAT + 1;
     __shared__ double red[32 * kRedStride];
     __shared__ double tot[16];
     const int b = blockIdx.y;
-    const int g = blockIdx.x * kStreamTile + threadIdx.x;
+    int at, g;
+    stream_site<NAT>(at, g);
     if (s == 1 && with_obs && blockIdx.x == 0) stream_reduce<NAT>(a, b, n, tot);
     double f1, f2;
     stream_drive(a, b, n, s, f1, f2);
@@ -142,17 +253,20 @@ stream_stage_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_c
     for (int q = 0; q < NR; ++q) o[q] = 0.0;
     if (g < a.G) {
         const double* yin = Yin.at(b);
-        if (s == 0 && with_obs)
-            rk4_stage_cell<NAT, Z, LZ, 2>(cp, a.nbr, a.G, g, a.dt, s, yin, y.at(b), acc.at(b), Ynext.at(b), nullptr,
-                                          f1, f2, drive, o);
-        else
-            rk4_stage_cell<NAT, Z, LZ, 0>(cp, a.nbr, a.G, g, a.dt, s, yin, y.at(b), acc.at(b), Ynext.at(b), nullptr,
-                                          f1, f2, drive, nullptr);
-        if (s == 0 && a.ckpt && n % a.ckpt_every == 0) {
-            double* dst = a.ckpt + ((long long)b * a.n_ckpt + n / a.ckpt_every) * a.V;
+        with_atom<NAT>(at, [&](auto tag) {
+            constexpr int AT = decltype(tag)::value;
+            if (s == 0 && with_obs)
+                rk4_stage_site<NAT, Z, LZ, AT, 2>(cp, a.nbr, a.G, g, a.dt, s, yin, y.at(b), acc.at(b), Ynext.at(b),
+                                                  f1, f2, drive, o);
+            else
+                rk4_stage_site<NAT, Z, LZ, AT, 0>(cp, a.nbr, a.G, g, a.dt, s, yin, y.at(b), acc.at(b), Ynext.at(b),
+                                                  f1, f2, drive, nullptr);
+            if (s == 0 && a.ckpt && n % a.ckpt_every == 0) {
+                double* dst = a.ckpt + ((long long)b * a.n_ckpt + n / a.ckpt_every) * a.V;
 #pragma unroll
-            for (int e = 0; e < NAT * 3; ++e) dst[(long long)e * a.G + g] = yin[(long long)e * a.G + g];
-        }
+                for (int c = 0; c < 3; ++c) dst[(long long)(AT * 3 + c) * a.G + g] = yin[(long long)(AT * 3 + c) * a.G + g];
+            }
+        });
     }
     if (s == 0 && with_obs) stream_store_partial<NR>(a, b, o, red, tot);
 }
@@ -165,14 +279,17 @@ stream_obs_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_con
     __shared__ double red[32 * kRedStride];
     __shared__ double tot[16];
     const int b = blockIdx.y;
-    const int g = blockIdx.x * kStreamTile + threadIdx.x;
+    int at, g;
+    stream_site<NAT>(at, g);
     double o[NR];
 #pragma unroll
     for (int q = 0; q < NR; ++q) o[q] = 0.0;
     if (g < a.G) {
         // a stage-3 pass with no output: only the observables of y are kept
-        rk4_stage_cell<NAT, Z, LZ, 2>(cp, a.nbr, a.G, g, a.dt, 3, y.at(b), y.at(b), nullptr, nullptr, nullptr, 0.0,
-                                      0.0, false, o);
+        with_atom<NAT>(at, [&](auto tag) {
+            rk4_stage_site<NAT, Z, LZ, decltype(tag)::value, 2>(cp, a.nbr, a.G, g, a.dt, 3, y.at(b), y.at(b), nullptr,
+                                                                nullptr, 0.0, 0.0, false, o);
+        });
     }
     stream_store_partial<NR>(a, b, o, red, tot);
 }
@@ -216,7 +333,7 @@ __global__ void stream_store_kernel(SVec y, int G, double* __restrict__ out) {
 // Adjoint sweep.
 
 struct StreamVjpArgs {
-    int G, tiles;
+    int G, tiles;                    // tiles of kStreamTile cells
     const int* nbr;
     double dt;
     long long n_steps;
@@ -241,8 +358,9 @@ __global__ void stream_lam_init_kernel(const __grid_constant__ StreamVjpArgs a, 
         for (int c = 0; c < 3; ++c) l[(at * 3 + c) * a.G + g] = 2.0 * (a.mloc[i + c] - a.target[i + c]) / a.n_sites;
 }
 
-// One stage VJP (stage s of step n) for every (tile, trajectory): mode and
-// buffers as vjp_cell; the tile's parameter cotangents are added to its slot.
+// One stage VJP (stage s of step n) for every (tile of kStreamTile cells,
+// trajectory), one cell per thread: mode and buffers as vjp_cell; the tile's
+// parameter cotangents are added to its slot.
 template <int NAT, int Z, int LZ, int NQ>
 __global__ void __launch_bounds__(kStreamTile)
 stream_vjp_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_constant__ ParamDerivs<NAT, Z, NQ> pd,
@@ -251,7 +369,7 @@ stream_vjp_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_con
     __shared__ double red[32 * kRedStride];
     __shared__ double tot[16];
     const int b = blockIdx.y;
-    const int g = blockIdx.x * kStreamTile + threadIdx.x;
+    const int g = blockIdx.x * kStreamTile + threadIdx.x;    // one cell per thread
     double f1 = 0.0, f2 = 0.0;
     if (a.drive) {
         const int q = s == 0 ? 0 : (s < 3 ? 2 : 4);
@@ -269,9 +387,10 @@ stream_vjp_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_con
     double gq[NQ];
 #pragma unroll
     for (int q = 0; q < NQ; ++q) gq[q] = 0.0;
-    if (g < a.G)
+    if (g < a.G) {
         vjp_cell<NAT, Z, LZ, NQ>(cp, pd, a.nbr, a.G, g, Y.at(b), lam.at(b), Sprev.at(b), ca, cb, f1, f2, drive,
                                  Sout.at(b), acc.at(b), lam_out.at(b), mode, dl, gq);
+    }
     double v[16];
 #pragma unroll
     for (int q = 0; q < 16; ++q) v[q] = q < NQ ? gq[q] : 0.0;

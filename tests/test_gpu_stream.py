@@ -82,7 +82,7 @@ def test_streamed_pyrochlore_integrate_with_states(api, oracle):
 
 
 def test_streamed_adjoint_kitaev_matches_tlm(native, oracle):
-    """24x24 honeycomb (576 cells: 3 tiles), two trajectories: streamed forward, recompute and VJP."""
+    """24x24 honeycomb (576 cells: 5 tiles of 128), two trajectories: streamed forward, recompute and VJP."""
     from classical_mcmc_spin_b200 import adjoint as adj
     theta = np.array([-1.0, 0.25, -0.02, 0.05, 0.1])
     build = lambda th: adj.kitaev_lattice(th, 24, 24)
@@ -107,7 +107,7 @@ def test_streamed_adjoint_kitaev_matches_tlm(native, oracle):
 
 
 def test_streamed_adjoint_pyrochlore_matches_tlm(native, oracle):
-    """Pyrochlore 5^3 conventional cells (2000 spins, 500 cells: 2 tiles) with a [111] field."""
+    """Pyrochlore 5^3 conventional cells (2000 spins, 500 cells: 8 tiles of 64) with a [111] field."""
     from classical_mcmc_spin_b200 import adjoint as adj
     theta = np.array([1.0, 0.05, 0.02, 0.2])
     build = lambda th: adj.pyrochlore_lattice(th, 5, 5, 5, cubic=True)
