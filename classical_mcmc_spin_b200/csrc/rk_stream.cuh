@@ -217,18 +217,32 @@ __device__ void stream_reduce(const StreamArgs& a, int b, long long n, double* s
     __syncthreads();
 }
 
+// Block sum of v[0..used) in a fixed order (lanes by the butterfly, then the
+// warps in order), finished in parallel: thread q < used gets the total of
+// value q and returns it in *out (other threads: false).
+template <int NV>
+__device__ __forceinline__ bool block_sum_par(double (&v)[NV], double* red, int used, double* out) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const double r = warp_reduce_many<NV>(v);
+    constexpr int span = 32 / NV;
+    if ((lane % span) == 0) red[warp * kRedStride + lane / span] = r;
+    __syncthreads();
+    if ((int)threadIdx.x >= used) return false;
+    double s = 0.0;
+    for (int w = 0; w < nw; ++w) s += red[w * kRedStride + threadIdx.x];
+    *out = s;
+    return true;
+}
+
 // Block-reduces this thread's partial o[NR] and stores it in the tile's slot.
 template <int NR>
 __device__ __forceinline__ void stream_store_partial(const StreamArgs& a, int b, const double (&o)[NR],
-                                                     double* red, double* tot) {
+                                                     double* red) {
     double v[16];
 #pragma unroll
     for (int q = 0; q < 16; ++q) v[q] = q < NR ? o[q] : 0.0;
-    block_sum<16>(v, red, NR, tot);
-    if (threadIdx.x == 0) {
-        double* p = a.part + ((long long)b * a.tiles + blockIdx.x) * kPart;
-        for (int q = 0; q < NR; ++q) p[q] = tot[q];
-    }
+    double t;
+    if (block_sum_par<16>(v, red, NR, &t)) a.part[((long long)b * a.tiles + blockIdx.x) * kPart + threadIdx.x] = t;
 }
 
 // One RK4 stage s of step n for every (tile, trajectory).  Stage 0 also leaves
@@ -268,7 +282,7 @@ stream_stage_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_c
             }
         });
     }
-    if (s == 0 && with_obs) stream_store_partial<NR>(a, b, o, red, tot);
+    if (s == 0 && with_obs) stream_store_partial<NR>(a, b, o, red);
 }
 
 // Observables' partials of y (the state after the last step).
@@ -277,7 +291,6 @@ __global__ void __launch_bounds__(kStreamTile)
 stream_obs_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_constant__ StreamArgs a, SVec y) {
     constexpr int NR = 3 * NAT + 1;
     __shared__ double red[32 * kRedStride];
-    __shared__ double tot[16];
     const int b = blockIdx.y;
     int at, g;
     stream_site<NAT>(at, g);
@@ -291,7 +304,7 @@ stream_obs_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_con
                                                                 nullptr, 0.0, 0.0, false, o);
         });
     }
-    stream_store_partial<NR>(a, b, o, red, tot);
+    stream_store_partial<NR>(a, b, o, red);
 }
 
 // Finishes step n's observables (one CTA per trajectory).
@@ -362,12 +375,11 @@ __global__ void stream_lam_init_kernel(const __grid_constant__ StreamVjpArgs a, 
 // trajectory), one cell per thread: mode and buffers as vjp_cell; the tile's
 // parameter cotangents are added to its slot.
 template <int NAT, int Z, int LZ, int NQ>
-__global__ void __launch_bounds__(kStreamTile)
+__global__ void __launch_bounds__(kStreamTile, 3)
 stream_vjp_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_constant__ ParamDerivs<NAT, Z, NQ> pd,
                   const __grid_constant__ StreamVjpArgs a, int s, long long n, SVec Y, SVec lam, SVec Sprev,
                   double ca, double cb, SVec Sout, SVec acc, SVec lam_out, int mode) {
     __shared__ double red[32 * kRedStride];
-    __shared__ double tot[16];
     const int b = blockIdx.y;
     const int g = blockIdx.x * kStreamTile + threadIdx.x;    // one cell per thread
     double f1 = 0.0, f2 = 0.0;
@@ -394,11 +406,8 @@ stream_vjp_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_con
     double v[16];
 #pragma unroll
     for (int q = 0; q < 16; ++q) v[q] = q < NQ ? gq[q] : 0.0;
-    block_sum<16>(v, red, NQ, tot);
-    if (threadIdx.x == 0) {
-        double* p = a.gpart + ((long long)b * a.tiles + blockIdx.x) * kPart;
-        for (int q = 0; q < NQ; ++q) p[q] += tot[q];
-    }
+    double t;
+    if (block_sum_par<16>(v, red, NQ, &t)) a.gpart[((long long)b * a.tiles + blockIdx.x) * kPart + threadIdx.x] += t;
 }
 
 // grad[b][q] = sum over tiles of the partials (tile order); one CTA per trajectory.
