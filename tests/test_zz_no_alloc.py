@@ -50,6 +50,7 @@ def _run(native, fn_name, h, lat, states, pulse4, n_steps, save, stream):
     desc.pulse4 = pulse4.data_ptr()
     launches = C.c_int32()
     fn = getattr(native.lib(), fn_name)
+    torch.cuda.synchronize()           # inputs and output fills written on torch's stream are complete
     native.check(fn(h.ptr, C.byref(desc), C.c_void_p(stream.cuda_stream), C.byref(launches)), fn_name)
     stream.synchronize()
     return obs.cpu().numpy(), fin.cpu().numpy(), launches.value
