@@ -56,8 +56,9 @@ def scan_workload(n_steps: int, rank: int = 0, world: int = 1):
     s0 = zigzag_honeycomb(L_SIDE, L_SIDE, 1, tilt_sigma=0.05, seed=2).ravel()
     fin = np.tile(np.ones(3) / np.sqrt(3.0), 2)
     fd = lat.rotate_pulse(fin, fin)
-    # weak scaling: rank r scans the delays shifted by r/world of one delay step
-    taus = 100.0 * (np.arange(N_DELAYS) + rank / world) / (N_DELAYS - 1)
+    # weak scaling: rank r scans its interleaved share of a world x 256 delay scan
+    from classical_mcmc_spin_b200.sharding import scan_delays
+    taus = scan_delays(N_DELAYS, 100.0, rank, world)
     pulses = []
     for tau in taus:
         for a1, a2 in ((0.5, 0.0), (0.0, 0.5), (0.5, 0.5)):
@@ -393,6 +394,7 @@ def main():
 
     from classical_mcmc_spin_b200 import _native as nat
     from classical_mcmc_spin_b200 import gpu_api
+    from classical_mcmc_spin_b200.sharding import max_over_ranks
 
     wl = scan_workload(args.md_steps, rank, world)
     lat = wl["lat"]
@@ -465,9 +467,7 @@ def main():
     total_ms = t_start.elapsed_time(t_end)
     kern_ms = [a.elapsed_time(b) for a, b in ev]
     if dist is not None:
-        tt = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+        total_ms = max_over_ranks(total_ms, dist, dev)
         dist.barrier()
     ms_per_step = total_ms / args.steps
     value = world * B * N * S / (ms_per_step * 1e-3)
@@ -509,9 +509,7 @@ def main():
         torch.cuda.synchronize(dev)
         e2e_s = (time.perf_counter() - t0) / n_e2e
         if dist is not None:
-            tt = torch.tensor([e2e_s], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e2e_s = float(tt.item())
+            e2e_s = max_over_ranks(e2e_s, dist, dev)
         e2e = {"value": world * B * N * S / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(h_init.numel() * 8 + P.size * 8),
                "d2h_bytes_per_step": int(h_obs.numel() * 8)}
