@@ -100,6 +100,21 @@ struct NVals {
     static constexpr int value = used <= 4 ? 4 : (used <= 8 ? 8 : (used <= 16 ? 16 : 32));
 };
 
+// h += j0*p0 + j1*p1 + j2*p2 as a chain of three fused multiply-adds (one
+// rounding per term; the plain expression costs a DMUL, two DFMAs and a DADD).
+__device__ __forceinline__ void bond_acc(double& h, double j0, double j1, double j2, double p0, double p1,
+                                         double p2) {
+    h = fma(j0, p0, h);
+    h = fma(j1, p1, h);
+    h = fma(j2, p2, h);
+}
+
+// h -= d1*f1 + d2*f2 as two fused multiply-adds.
+__device__ __forceinline__ void drive_acc(double& h, double d1, double d2, double f1, double f2) {
+    h = fma(-d1, f1, h);
+    h = fma(-d2, f2, h);
+}
+
 // Drive envelope of lattice_md.cpp:45-56: a * exp(-(x/(2w))^2) * cos(freq x).
 __device__ __forceinline__ double drive_factor(double amp, double x, double width, double freq) {
     const double u = x / (2.0 * width);
@@ -226,19 +241,17 @@ rk4_resident_kernel(const __grid_constant__ Couplings<NAT, Z> cp,
         }
         if (cp.has_onsite) {
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                H[d] += 2.0 * cp.onsite[at][3 * d + 0] * S[at][0];
-                H[d] += 2.0 * cp.onsite[at][3 * d + 1] * S[at][1];
-                H[d] += 2.0 * cp.onsite[at][3 * d + 2] * S[at][2];
-            }
+            for (int d = 0; d < 3; ++d)
+                bond_acc(H[d], 2.0 * cp.onsite[at][3 * d], 2.0 * cp.onsite[at][3 * d + 1],
+                         2.0 * cp.onsite[at][3 * d + 2], S[at][0], S[at][1], S[at][2]);
         }
 #pragma unroll
         for (int n = 0; n < LZ; ++n) {
             const int pb = (at + 1 + n) % NAT;
 #pragma unroll
             for (int d = 0; d < 3; ++d)
-                H[d] += cp.J[at][n][3 * d] * S[pb][0] + cp.J[at][n][3 * d + 1] * S[pb][1] +
-                        cp.J[at][n][3 * d + 2] * S[pb][2];
+                bond_acc(H[d], cp.J[at][n][3 * d], cp.J[at][n][3 * d + 1], cp.J[at][n][3 * d + 2], S[pb][0],
+                         S[pb][1], S[pb][2]);
         }
 #pragma unroll
         for (int m = 0; m < NL; ++m) {
@@ -248,7 +261,7 @@ rk4_resident_kernel(const __grid_constant__ Couplings<NAT, Z> cp,
                 const double P0 = smem[p], P1 = smem[p + G], P2 = smem[p + 2 * G];
 #pragma unroll
                 for (int d = 0; d < 3; ++d)
-                    H[d] += cp.J[at][n][3 * d] * P0 + cp.J[at][n][3 * d + 1] * P1 + cp.J[at][n][3 * d + 2] * P2;
+                    bond_acc(H[d], cp.J[at][n][3 * d], cp.J[at][n][3 * d + 1], cp.J[at][n][3 * d + 2], P0, P1, P2);
             }
         }
     };
@@ -332,7 +345,7 @@ rk4_resident_kernel(const __grid_constant__ Couplings<NAT, Z> cp,
                     }
                     if (drive_now) {
 #pragma unroll
-                        for (int d = 0; d < 3; ++d) H[d] -= cp.d1[at][d] * f1 + cp.d2[at][d] * f2;
+                        for (int d = 0; d < 3; ++d) drive_acc(H[d], cp.d1[at][d], cp.d2[at][d], f1, f2);
                     }
                     const double kk[3] = {H[1] * S[at][2] - H[2] * S[at][1], H[2] * S[at][0] - H[0] * S[at][2],
                                           H[0] * S[at][1] - H[1] * S[at][0]};

@@ -116,9 +116,7 @@ __device__ __forceinline__ void rk4_stage_cell(const Couplings<NAT, Z>& cp, cons
         if (cp.has_onsite) {
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
-                H[d] += 2.0 * cp.onsite[at][3 * d + 0] * S[at][0];
-                H[d] += 2.0 * cp.onsite[at][3 * d + 1] * S[at][1];
-                H[d] += 2.0 * cp.onsite[at][3 * d + 2] * S[at][2];
+                bond_acc(H[d], 2.0 * cp.onsite[at][3 * d], 2.0 * cp.onsite[at][3 * d + 1], 2.0 * cp.onsite[at][3 * d + 2], S[at][0], S[at][1], S[at][2]);
             }
         }
 #pragma unroll
@@ -126,8 +124,7 @@ __device__ __forceinline__ void rk4_stage_cell(const Couplings<NAT, Z>& cp, cons
             const int pb = (at + 1 + n) % NAT;
 #pragma unroll
             for (int d = 0; d < 3; ++d)
-                H[d] += cp.J[at][n][3 * d] * S[pb][0] + cp.J[at][n][3 * d + 1] * S[pb][1] +
-                        cp.J[at][n][3 * d + 2] * S[pb][2];
+                bond_acc(H[d], cp.J[at][n][3 * d], cp.J[at][n][3 * d + 1], cp.J[at][n][3 * d + 2], S[pb][0], S[pb][1], S[pb][2]);
         }
 #pragma unroll
         for (int mm = 0; mm < NL; ++mm) {
@@ -137,7 +134,7 @@ __device__ __forceinline__ void rk4_stage_cell(const Couplings<NAT, Z>& cp, cons
                 const double P0 = Yin[p], P1 = Yin[p + G], P2 = Yin[p + 2 * G];
 #pragma unroll
                 for (int d = 0; d < 3; ++d)
-                    H[d] += cp.J[at][n][3 * d] * P0 + cp.J[at][n][3 * d + 1] * P1 + cp.J[at][n][3 * d + 2] * P2;
+                    bond_acc(H[d], cp.J[at][n][3 * d], cp.J[at][n][3 * d + 1], cp.J[at][n][3 * d + 2], P0, P1, P2);
             }
         }
         if (OBS == 2) {          // twice the energy: S.(H_static - B), before the drive enters
@@ -146,7 +143,7 @@ __device__ __forceinline__ void rk4_stage_cell(const Couplings<NAT, Z>& cp, cons
         }
         if (drive) {
 #pragma unroll
-            for (int d = 0; d < 3; ++d) H[d] -= cp.d1[at][d] * f1 + cp.d2[at][d] * f2;
+            for (int d = 0; d < 3; ++d) drive_acc(H[d], cp.d1[at][d], cp.d2[at][d], f1, f2);
         }
         if (Hout) {
 #pragma unroll
@@ -302,9 +299,7 @@ __device__ __forceinline__ void vjp_cell(const Couplings<NAT, Z>& cp, const Para
         if (cp.has_onsite) {
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
-                H[d] += 2.0 * cp.onsite[at][3 * d + 0] * S0;
-                H[d] += 2.0 * cp.onsite[at][3 * d + 1] * S1;
-                H[d] += 2.0 * cp.onsite[at][3 * d + 2] * S2;
+                bond_acc(H[d], 2.0 * cp.onsite[at][3 * d], 2.0 * cp.onsite[at][3 * d + 1], 2.0 * cp.onsite[at][3 * d + 2], S0, S1, S2);
                 sb[d] += 2.0 * (cp.onsite[at][d] * hown[0] + cp.onsite[at][3 + d] * hown[1] +
                                 cp.onsite[at][6 + d] * hown[2]);
             }
@@ -324,8 +319,8 @@ __device__ __forceinline__ void vjp_cell(const Couplings<NAT, Z>& cp, const Para
         auto bond = [&](int n, const double (&P)[3], const double (&Q)[3]) {
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
-                H[d] += cp.J[at][n][3 * d] * P[0] + cp.J[at][n][3 * d + 1] * P[1] + cp.J[at][n][3 * d + 2] * P[2];
-                sb[d] += cp.J[at][n][3 * d] * Q[0] + cp.J[at][n][3 * d + 1] * Q[1] + cp.J[at][n][3 * d + 2] * Q[2];
+                bond_acc(H[d], cp.J[at][n][3 * d], cp.J[at][n][3 * d + 1], cp.J[at][n][3 * d + 2], P[0], P[1], P[2]);
+                bond_acc(sb[d], cp.J[at][n][3 * d], cp.J[at][n][3 * d + 1], cp.J[at][n][3 * d + 2], Q[0], Q[1], Q[2]);
             }
 #pragma unroll
             for (int q = 0; q < NQ; ++q) {
@@ -353,7 +348,7 @@ __device__ __forceinline__ void vjp_cell(const Couplings<NAT, Z>& cp, const Para
         }
         if (drive) {
 #pragma unroll
-            for (int d = 0; d < 3; ++d) H[d] -= cp.d1[at][d] * f1 + cp.d2[at][d] * f2;
+            for (int d = 0; d < 3; ++d) drive_acc(H[d], cp.d1[at][d], cp.d2[at][d], f1, f2);
         }
         double v[3];
         cot(i0, v);

@@ -83,9 +83,7 @@ __device__ __forceinline__ void rhs_cell(const Couplings<NAT, Z>& cp, const doub
         if (cp.has_onsite) {
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
-                H[d] += 2.0 * cp.onsite[at][3 * d + 0] * S[at][0];
-                H[d] += 2.0 * cp.onsite[at][3 * d + 1] * S[at][1];
-                H[d] += 2.0 * cp.onsite[at][3 * d + 2] * S[at][2];
+                bond_acc(H[d], 2.0 * cp.onsite[at][3 * d], 2.0 * cp.onsite[at][3 * d + 1], 2.0 * cp.onsite[at][3 * d + 2], S[at][0], S[at][1], S[at][2]);
             }
         }
 #pragma unroll
@@ -93,8 +91,7 @@ __device__ __forceinline__ void rhs_cell(const Couplings<NAT, Z>& cp, const doub
             const int pb = (at + 1 + n) % NAT;
 #pragma unroll
             for (int d = 0; d < 3; ++d)
-                H[d] += cp.J[at][n][3 * d] * S[pb][0] + cp.J[at][n][3 * d + 1] * S[pb][1] +
-                        cp.J[at][n][3 * d + 2] * S[pb][2];
+                bond_acc(H[d], cp.J[at][n][3 * d], cp.J[at][n][3 * d + 1], cp.J[at][n][3 * d + 2], S[pb][0], S[pb][1], S[pb][2]);
         }
 #pragma unroll
         for (int m = 0; m < NL; ++m) {
@@ -104,7 +101,7 @@ __device__ __forceinline__ void rhs_cell(const Couplings<NAT, Z>& cp, const doub
                 const double P0 = Y[p], P1 = Y[p + G], P2 = Y[p + 2 * G];
 #pragma unroll
                 for (int d = 0; d < 3; ++d)
-                    H[d] += cp.J[at][n][3 * d] * P0 + cp.J[at][n][3 * d + 1] * P1 + cp.J[at][n][3 * d + 2] * P2;
+                    bond_acc(H[d], cp.J[at][n][3 * d], cp.J[at][n][3 * d + 1], cp.J[at][n][3 * d + 2], P0, P1, P2);
             }
         }
         if (part) {
@@ -114,7 +111,7 @@ __device__ __forceinline__ void rhs_cell(const Couplings<NAT, Z>& cp, const doub
         }
         if (drive) {
 #pragma unroll
-            for (int d = 0; d < 3; ++d) H[d] -= cp.d1[at][d] * f1 + cp.d2[at][d] * f2;
+            for (int d = 0; d < 3; ++d) drive_acc(H[d], cp.d1[at][d], cp.d2[at][d], f1, f2);
         }
         K[(at * 3 + 0) * G + g] = H[1] * S[at][2] - H[2] * S[at][1];
         K[(at * 3 + 1) * G + g] = H[2] * S[at][0] - H[0] * S[at][2];

@@ -114,9 +114,7 @@ __device__ __forceinline__ void rk4_stage_site(const Couplings<NAT, Z>& cp, cons
     if (cp.has_onsite) {
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            H[d] += 2.0 * cp.onsite[AT][3 * d + 0] * S[0];
-            H[d] += 2.0 * cp.onsite[AT][3 * d + 1] * S[1];
-            H[d] += 2.0 * cp.onsite[AT][3 * d + 2] * S[2];
+            bond_acc(H[d], 2.0 * cp.onsite[AT][3 * d], 2.0 * cp.onsite[AT][3 * d + 1], 2.0 * cp.onsite[AT][3 * d + 2], S[0], S[1], S[2]);
         }
     }
 #pragma unroll
@@ -125,7 +123,7 @@ __device__ __forceinline__ void rk4_stage_site(const Couplings<NAT, Z>& cp, cons
         const double P0 = Yin[ip], P1 = Yin[ip + G], P2 = Yin[ip + 2 * G];
 #pragma unroll
         for (int d = 0; d < 3; ++d)
-            H[d] += cp.J[AT][n][3 * d] * P0 + cp.J[AT][n][3 * d + 1] * P1 + cp.J[AT][n][3 * d + 2] * P2;
+            bond_acc(H[d], cp.J[AT][n][3 * d], cp.J[AT][n][3 * d + 1], cp.J[AT][n][3 * d + 2], P0, P1, P2);
     }
 #pragma unroll
     for (int m = 0; m < NL; ++m) {
@@ -135,7 +133,7 @@ __device__ __forceinline__ void rk4_stage_site(const Couplings<NAT, Z>& cp, cons
             const double P0 = Yin[p], P1 = Yin[p + G], P2 = Yin[p + 2 * G];
 #pragma unroll
             for (int d = 0; d < 3; ++d)
-                H[d] += cp.J[AT][n][3 * d] * P0 + cp.J[AT][n][3 * d + 1] * P1 + cp.J[AT][n][3 * d + 2] * P2;
+                bond_acc(H[d], cp.J[AT][n][3 * d], cp.J[AT][n][3 * d + 1], cp.J[AT][n][3 * d + 2], P0, P1, P2);
         }
     }
     if (OBS == 2) {
@@ -146,7 +144,7 @@ __device__ __forceinline__ void rk4_stage_site(const Couplings<NAT, Z>& cp, cons
     }
     if (drive) {
 #pragma unroll
-        for (int d = 0; d < 3; ++d) H[d] -= cp.d1[AT][d] * f1 + cp.d2[AT][d] * f2;
+        for (int d = 0; d < 3; ++d) drive_acc(H[d], cp.d1[AT][d], cp.d2[AT][d], f1, f2);
     }
     const double k[3] = {H[1] * S[2] - H[2] * S[1], H[2] * S[0] - H[0] * S[2], H[0] * S[1] - H[1] * S[0]};
     const double cy = s == 2 ? dt : 0.5 * dt;
