@@ -304,22 +304,24 @@ void fill_couplings(const cmd_handle* h, const double* d1, const double* d2, cmd
     cp.has_onsite = h->has_onsite;
 }
 
-size_t resident_smem(int NA, int64_t G) {
-    return (size_t)2 * NA * 3 * G * sizeof(double) + (32 * cmd::kRedStride + 12) * sizeof(double);
+// Shared memory of the resident kernel: two stage buffers per trajectory of a
+// CTA, the reduction rows and the staged envelopes.
+size_t resident_smem(int NA, int64_t G, int tpc = 1) {
+    return (size_t)tpc * 2 * NA * 3 * G * sizeof(double) + (32 * cmd::kRedStride + 12 * tpc) * sizeof(double);
 }
 
 using LaunchFn = int (*)(const cmd_handle*, const cmd::ResidentArgs&, const double*, const double*, int64_t,
                          cudaStream_t);
 
-template <int NAT, int Z, int LZ, int CPT, int MAXT, int MINB, bool YREG>
+template <int NAT, int Z, int LZ, int CPT, int MAXT, int MINB, bool YREG, int TPC>
 int launch_one(const cmd_handle* h, const cmd::ResidentArgs& args, const double* d1, const double* d2,
                int64_t B, cudaStream_t st) {
-    auto kern = cmd::rk4_resident_kernel<NAT, Z, LZ, CPT, MAXT, MINB, YREG>;
+    auto kern = cmd::rk4_resident_kernel<NAT, Z, LZ, CPT, MAXT, MINB, YREG, TPC>;
     const int64_t G = h->lay.G;
     int threads = (int)((G + CPT - 1) / CPT);
     threads = ((threads + 31) / 32) * 32;
     if (threads > MAXT) return fail(CMD_ERR_UNSUPPORTED, "lattice too large for this kernel variant");
-    const size_t smem = resident_smem(NAT, G);
+    const size_t smem = resident_smem(NAT, G, TPC);
     if (smem > kMaxSmem) return fail(CMD_ERR_UNSUPPORTED, "stage buffers exceed shared memory");
     static bool attr_set = false;
     if (!attr_set) {
@@ -328,39 +330,48 @@ int launch_one(const cmd_handle* h, const cmd::ResidentArgs& args, const double*
     }
     cmd::Couplings<NAT, Z> cp;
     fill_couplings<NAT, Z>(h, d1, d2, cp);
-    kern<<<(unsigned)B, threads, smem, st>>>(cp, args);
+    cmd::ResidentArgs a = args;
+    a.B = B;
+    kern<<<(unsigned)((B + TPC - 1) / TPC), threads, smem, st>>>(cp, a);
     CUDA_TRY(cudaGetLastError());
     return CMD_OK;
 }
 
 // Resident-kernel variants compiled into the library: (atoms/cell, bonds/atom,
 // in-cell bonds) x (cells per thread, max threads, min CTAs per SM, own stage
-// input kept in registers).  The autotuner times the ones that fit a lattice.
+// input kept in registers, trajectories per CTA).  The autotuner times the
+// ones that fit a lattice.
 struct Variant {
     int NAT, Z, LZ, CPT, MAXT, MINB;
     bool YREG;
+    int TPC;
     LaunchFn fn;
     const char* name;
 };
 
-#define CMD_VARIANT(NAT, Z, LZ, CPT, MAXT, MINB, YREG) \
-    Variant{NAT, Z, LZ, CPT, MAXT, MINB, YREG, &launch_one<NAT, Z, LZ, CPT, MAXT, MINB, YREG>, \
-            "rk4_resident<" #NAT "," #Z "," #LZ "> cpt=" #CPT " maxt=" #MAXT " minb=" #MINB " yreg=" #YREG}
+#define CMD_VARIANT(NAT, Z, LZ, CPT, MAXT, MINB, YREG, TPC) \
+    Variant{NAT, Z, LZ, CPT, MAXT, MINB, YREG, TPC, &launch_one<NAT, Z, LZ, CPT, MAXT, MINB, YREG, TPC>, \
+            "rk4_resident<" #NAT "," #Z "," #LZ "> cpt=" #CPT " maxt=" #MAXT " minb=" #MINB " yreg=" #YREG \
+            " tpc=" #TPC}
 
 const Variant kVariants[] = {
     // 2-atom cells with 3 bonds per site (Kitaev / Heisenberg honeycomb)
-    CMD_VARIANT(2, 3, 1, 1, 640, 1, true),
-    CMD_VARIANT(2, 3, 1, 2, 320, 2, false),
-    CMD_VARIANT(2, 3, 1, 3, 192, 3, false),
-    CMD_VARIANT(2, 3, 1, 4, 160, 3, false),
-    CMD_VARIANT(2, 3, 1, 4, 160, 3, true),
-    CMD_VARIANT(2, 3, 1, 6, 96, 3, true),
-    CMD_VARIANT(2, 3, 1, 2, 512, 1, true),
-    CMD_VARIANT(2, 3, 1, 4, 256, 2, false),
+    CMD_VARIANT(2, 3, 1, 1, 640, 1, true, 1),
+    CMD_VARIANT(2, 3, 1, 2, 320, 2, false, 1),
+    CMD_VARIANT(2, 3, 1, 3, 192, 3, false, 1),
+    CMD_VARIANT(2, 3, 1, 4, 160, 3, false, 1),
+    CMD_VARIANT(2, 3, 1, 4, 160, 3, true, 1),
+    CMD_VARIANT(2, 3, 1, 6, 96, 3, true, 1),
+    CMD_VARIANT(2, 3, 1, 2, 512, 1, true, 1),
+    CMD_VARIANT(2, 3, 1, 4, 256, 2, false, 1),
+    // two trajectories per CTA: twice the independent work between barriers
+    CMD_VARIANT(2, 3, 1, 1, 640, 1, false, 2),
+    CMD_VARIANT(2, 3, 1, 1, 640, 1, true, 2),
+    CMD_VARIANT(2, 3, 1, 2, 320, 1, false, 2),
     // 4-atom cells with 6 bonds per site (nearest-neighbour pyrochlore)
-    CMD_VARIANT(4, 6, 3, 1, 512, 1, true),
-    CMD_VARIANT(4, 6, 3, 2, 256, 2, false),
-    CMD_VARIANT(4, 6, 3, 2, 512, 1, false),
+    CMD_VARIANT(4, 6, 3, 1, 512, 1, true, 1),
+    CMD_VARIANT(4, 6, 3, 2, 256, 2, false, 1),
+    CMD_VARIANT(4, 6, 3, 2, 512, 1, false, 1),
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 
@@ -368,7 +379,7 @@ bool variant_fits(const Variant& v, const Layout& L) {
     if (!L.uniform || v.NAT != L.NA || v.Z != L.Z || v.LZ != L.LZ) return false;
     const int64_t threads = ((L.G + v.CPT - 1) / v.CPT + 31) / 32 * 32;
     if (threads > v.MAXT) return false;
-    const size_t smem = resident_smem(v.NAT, L.G);
+    const size_t smem = resident_smem(v.NAT, L.G, v.TPC);
     if (smem > kMaxSmem) return false;
     return true;
 }

@@ -55,6 +55,7 @@ struct Pulse {
 
 struct ResidentArgs {
     int G;                    // groups (cells) per trajectory
+    long long B;              // trajectories
     long long n_steps;
     long long save_every;
     double T0, dt;
@@ -176,63 +177,75 @@ __global__ void finish_rows_kernel(const double* raw, long long raw_stride, long
     }
 }
 
-template <int NAT, int Z, int LZ, int CPT, int MAXT, int MINB, bool YREG>
+template <int NAT, int Z, int LZ, int CPT, int MAXT, int MINB, bool YREG, int TPC>
 __global__ void __launch_bounds__(MAXT, MINB)
 rk4_resident_kernel(const __grid_constant__ Couplings<NAT, Z> cp,
                     const __grid_constant__ ResidentArgs a) {
     constexpr int NL = Z - LZ;                       // non-local slots per atom
-    constexpr int NV = NVals<NAT>::value;
-    constexpr int NR = NVals<NAT>::used;
+    constexpr int NR = NVals<NAT>::used;             // observables per trajectory
+    constexpr int NRT = NR * TPC;                    // observables of the CTA's trajectories
+    constexpr int NV = NRT <= 4 ? 4 : (NRT <= 8 ? 8 : 16);
+    static_assert(NRT <= kRedStride, "observables of a CTA must fit one reduction row");
     extern __shared__ double smem[];
     const int G = a.G;
     const int SB = NAT * 3 * G;                      // one stage buffer
-    // Shared memory is addressed through 32-bit offsets (stage buffers at 0
-    // and SB), which keeps the addressing in the shared window and in 32-bit
-    // registers.
-    double* red = smem + 2 * SB;                     // [32][kRedStride]
-    double* drv = red + 32 * kRedStride;             // [2][6] envelopes of the current / next step
+    // Trajectory t of this CTA keeps its two stage buffers at t*2*SB (+ 0 / SB).
+    // Shared memory is addressed through 32-bit offsets, which keeps the
+    // addressing in the shared window and in 32-bit registers.
+    double* red = smem + TPC * 2 * SB;               // [32][kRedStride]
+    double* drv = red + 32 * kRedStride;             // [TPC][2][6] envelopes of the current / next step
 
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-    const long long b = blockIdx.x;
+    const long long b0 = (long long)blockIdx.x * TPC;
+    const int ntr = (int)(a.B - b0 < TPC ? a.B - b0 : TPC);   // trajectories of this CTA (uniform)
 
-    double y[CPT][NAT][3], acc[CPT][NAT][3];
-    double yc[YREG ? CPT : 1][NAT][3];
+    double y[TPC][CPT][NAT][3], acc[TPC][CPT][NAT][3];
+    double yc[YREG ? TPC : 1][YREG ? CPT : 1][NAT][3];
     int nb[CPT][NAT][NL > 0 ? NL : 1];
 
-    const double* y0 = a.y0 + b * a.y0_stride;
+#pragma unroll
+    for (int t = 0; t < TPC; ++t) {
+        const double* y0 = a.y0 + (b0 + t) * a.y0_stride;
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            const int g = tid + k * blockDim.x;
+            const bool own = g < G && t < ntr;
+#pragma unroll
+            for (int at = 0; at < NAT; ++at)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const double v = own ? y0[((long long)g * NAT + at) * 3 + c] : 0.0;
+                    y[t][k][at][c] = v;
+                    if (YREG) yc[YREG ? t : 0][YREG ? k : 0][at][c] = v;
+                    acc[t][k][at][c] = 0.0;
+                    if (own) smem[t * 2 * SB + (at * 3 + c) * G + g] = v;
+                }
+        }
+    }
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
         const int g = tid + k * blockDim.x;
-        const bool own = g < G;
 #pragma unroll
-        for (int at = 0; at < NAT; ++at) {
+        for (int at = 0; at < NAT; ++at)
 #pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const double v = own ? y0[((long long)g * NAT + at) * 3 + c] : 0.0;
-                y[k][at][c] = v;
-                if (YREG) yc[YREG ? k : 0][at][c] = v;
-                acc[k][at][c] = 0.0;
-                if (own) smem[(at * 3 + c) * G + g] = v;
-            }
-#pragma unroll
-            for (int m = 0; m < NL; ++m)
-                nb[k][at][m] = own ? a.nbr[((long long)g * NAT + at) * NL + m] : 0;
-        }
+            for (int m = 0; m < NL; ++m) nb[k][at][m] = g < G ? a.nbr[((long long)g * NAT + at) * NL + m] : 0;
     }
 
     const bool drive_on = a.drive != nullptr;
-    const double* dtab = drive_on ? a.drive + b * a.n_steps * 6 : nullptr;
     const double dt = a.dt;
-    // Lanes 0..5 of warp 0 stage the envelopes: loaded during stage 0 of step n
-    // for step n+1, stored to drv[] during stage 2, read by everyone after the
-    // stage-3 barrier.  Nothing waits on the global load.
-    const bool stager = drive_on && warp == 0 && lane < 6;
-    if (stager && a.n_steps > 0) drv[lane] = dtab[lane];
+    // Lanes 0..6*TPC-1 of warp 0 stage the envelopes (lane l: trajectory l/6,
+    // value l%6): loaded during stage 0 of step n for step n+1, stored to drv[]
+    // during stage 2, read by everyone after the stage-3 barrier.  Nothing
+    // waits on the global load.
+    const int st_t = lane / 6, st_e = lane - 6 * (lane / 6);
+    const bool stager = drive_on && warp == 0 && lane < 6 * TPC && st_t < ntr;
+    const double* dtab = stager ? a.drive + (b0 + st_t) * a.n_steps * 6 : nullptr;
+    if (stager && a.n_steps > 0) drv[st_t * 12 + st_e] = dtab[st_e];
     __syncthreads();
 
-    // Static field at the current stage input of cell k, atom at.  S[][] holds
-    // the cell's NAT stage-input spins.
+    // Static field at the current stage input (buffer offset `in`) of cell k,
+    // atom at.  S[][] holds the cell's NAT stage-input spins.
     auto field_at = [&](int in, int k, int at, const double (&S)[NAT][3], double (&H)[3]) {
         if (cp.has_field) {
             H[0] = -cp.field[at][0]; H[1] = -cp.field[at][1]; H[2] = -cp.field[at][2];
@@ -265,13 +278,13 @@ rk4_resident_kernel(const __grid_constant__ Couplings<NAT, Z> cp,
             }
         }
     };
-    auto load_cell = [&](int in, int k, double (&S)[NAT][3]) {
+    auto load_cell = [&](int in, int t, int k, double (&S)[NAT][3]) {
         const int g = tid + k * blockDim.x;
 #pragma unroll
         for (int at = 0; at < NAT; ++at)
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                if (YREG) S[at][c] = yc[YREG ? k : 0][at][c];
+                if (YREG) S[at][c] = yc[YREG ? t : 0][YREG ? k : 0][at][c];
                 else S[at][c] = smem[in + (at * 3 + c) * G + g];
             }
     };
@@ -282,135 +295,154 @@ rk4_resident_kernel(const __grid_constant__ Couplings<NAT, Z> cp,
         if ((lane % span) == 0) red[warp * kRedStride + lane / span] = r;
     };
     // Warp q sums value q (q = warp, warp + nwarps, ...) over the warps and
-    // writes it (runs after a barrier).
+    // writes it to its trajectory's row (runs after a barrier).
     auto finish_raw = [&](long long row) {
         if (a.raw == nullptr) return;
-        for (int q = warp; q < NR; q += nwarps) {
+        for (int q = warp; q < NRT; q += nwarps) {
             double s = lane < nwarps ? red[lane * kRedStride + q] : 0.0;
 #pragma unroll
             for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) a.raw[(b * a.rows + row) * a.raw_stride + q] = s;
+            const int t = q / NR;
+            if (lane == 0 && t < ntr) a.raw[((b0 + t) * a.rows + row) * a.raw_stride + (q - t * NR)] = s;
         }
     };
     auto write_traj = [&](long long row) {
         if (!a.traj) return;
-        double* dst = a.traj + (b * a.rows + row) * (long long)G * NAT * 3;
 #pragma unroll
-        for (int k = 0; k < CPT; ++k) {
-            const int g = tid + k * blockDim.x;
-            if (g >= G) continue;
+        for (int t = 0; t < TPC; ++t) {
+            if (t >= ntr) continue;
+            double* dst = a.traj + ((b0 + t) * a.rows + row) * (long long)G * NAT * 3;
 #pragma unroll
-            for (int at = 0; at < NAT; ++at)
+            for (int k = 0; k < CPT; ++k) {
+                const int g = tid + k * blockDim.x;
+                if (g >= G) continue;
 #pragma unroll
-                for (int c = 0; c < 3; ++c) dst[((long long)g * NAT + at) * 3 + c] = y[k][at][c];
+                for (int at = 0; at < NAT; ++at)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) dst[((long long)g * NAT + at) * 3 + c] = y[t][k][at][c];
+            }
         }
     };
 
     long long row = 0;
     long long save_left = 0;            // steps until the next saved row
-    bool pending = false;
-    int in = 0;          // offset of the buffer holding the current stage input
+    int in = 0;          // offset (within a trajectory's pair) of the buffer holding the current stage input
     int out = SB;
+    // Observables of step n: summed per thread during stage 0, warp-reduced at
+    // the start of stage 1 (off the stage-0 barrier's critical path, next to
+    // stage 1's own work), finished across warps and written in stage 2.
+    double part[NV];
     for (long long step = 0; step < a.n_steps; ++step) {
         const bool observe = save_left == 0;
         save_left = observe ? a.save_every - 1 : save_left - 1;
-        const double* dv = drv + 6 * (step & 1);
         double next_f = 0.0;
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
-            if (s == 0 && stager && step + 1 < a.n_steps) next_f = dtab[(step + 1) * 6 + lane];
-            if (s == 2 && stager && step + 1 < a.n_steps) drv[6 * ((step + 1) & 1) + lane] = next_f;
+            if (s == 0 && stager && step + 1 < a.n_steps) next_f = dtab[(step + 1) * 6 + st_e];
+            if (s == 2 && stager && step + 1 < a.n_steps) drv[st_t * 12 + 6 * ((step + 1) & 1) + st_e] = next_f;
             const int ti = s == 0 ? 0 : (s == 3 ? 2 : 1);
-            const double f1 = drive_on ? dv[2 * ti] : 0.0;
-            const double f2 = drive_on ? dv[2 * ti + 1] : 0.0;
-            const bool drive_now = drive_on && (f1 != 0.0 || f2 != 0.0);   // 0*d adds exactly 0
-            double part[NV];
+            if (s == 0) {
 #pragma unroll
-            for (int q = 0; q < NV; ++q) part[q] = 0.0;
-#pragma unroll
-            for (int k = 0; k < CPT; ++k) {
-                const int g = tid + k * blockDim.x;
-                if (g >= G) continue;
-                double S[NAT][3];
-                load_cell(in, k, S);
-                double nx[YREG ? NAT : 1][3];
-#pragma unroll
-                for (int at = 0; at < NAT; ++at) {
-                    double H[3];
-                    field_at(in, k, at, S, H);
-                    if (s == 0 && observe) {
-                        part[3 * at] += S[at][0]; part[3 * at + 1] += S[at][1]; part[3 * at + 2] += S[at][2];
-                        part[3 * NAT] += S[at][0] * (H[0] - cp.field[at][0]) + S[at][1] * (H[1] - cp.field[at][1]) +
-                                         S[at][2] * (H[2] - cp.field[at][2]);
-                    }
-                    if (drive_now) {
-#pragma unroll
-                        for (int d = 0; d < 3; ++d) drive_acc(H[d], cp.d1[at][d], cp.d2[at][d], f1, f2);
-                    }
-                    const double kk[3] = {H[1] * S[at][2] - H[2] * S[at][1], H[2] * S[at][0] - H[0] * S[at][2],
-                                          H[0] * S[at][1] - H[1] * S[at][0]};
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        double v;
-                        if (s == 0) {
-                            acc[k][at][c] = kk[c];
-                            v = 1.0 * y[k][at][c] + (0.5 * dt) * kk[c];
-                        } else if (s == 1) {
-                            acc[k][at][c] = acc[k][at][c] + 2.0 * kk[c];
-                            v = 1.0 * y[k][at][c] + (0.5 * dt) * kk[c];
-                        } else if (s == 2) {
-                            acc[k][at][c] = acc[k][at][c] + 2.0 * kk[c];
-                            v = 1.0 * y[k][at][c] + dt * kk[c];
-                        } else {
-                            y[k][at][c] += (dt / 6.0) * (acc[k][at][c] + kk[c]);
-                            v = y[k][at][c];
-                        }
-                        if (YREG) nx[YREG ? at : 0][c] = v;     // own registers change after the cell
-                        else smem[out + (at * 3 + c) * G + g] = v;
-                    }
-                }
-                if (YREG) {
-#pragma unroll
-                    for (int at = 0; at < NAT; ++at)
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) {
-                            yc[YREG ? k : 0][at][c] = nx[YREG ? at : 0][c];
-                            smem[out + (at * 3 + c) * G + g] = nx[YREG ? at : 0][c];
-                        }
-                }
+                for (int q = 0; q < NV; ++q) part[q] = 0.0;
             }
-            if (s == 0 && observe) {
-                write_traj(row);
-                reduce_partials(part);
-            }
-            if (s == 1 && pending) {
+            if (s == 1 && observe) reduce_partials(part);
+            if (s == 2 && observe) {
                 finish_raw(row);
                 ++row;
-                pending = false;
             }
+#pragma unroll
+            for (int t = 0; t < TPC; ++t) {
+                if (t >= ntr) continue;
+                const int tin = t * 2 * SB + in, tout = t * 2 * SB + out;
+                const double* dv = drv + t * 12 + 6 * (step & 1);
+                const double f1 = drive_on ? dv[2 * ti] : 0.0;
+                const double f2 = drive_on ? dv[2 * ti + 1] : 0.0;
+                const bool drive_now = drive_on && (f1 != 0.0 || f2 != 0.0);   // 0*d adds exactly 0
+#pragma unroll
+                for (int k = 0; k < CPT; ++k) {
+                    const int g = tid + k * blockDim.x;
+                    if (g >= G) continue;
+                    double S[NAT][3];
+                    load_cell(tin, t, k, S);
+                    double nx[YREG ? NAT : 1][3];
+#pragma unroll
+                    for (int at = 0; at < NAT; ++at) {
+                        double H[3];
+                        field_at(tin, k, at, S, H);
+                        if (s == 0 && observe) {
+                            part[t * NR + 3 * at] += S[at][0];
+                            part[t * NR + 3 * at + 1] += S[at][1];
+                            part[t * NR + 3 * at + 2] += S[at][2];
+                            part[t * NR + 3 * NAT] += S[at][0] * (H[0] - cp.field[at][0]) +
+                                                      S[at][1] * (H[1] - cp.field[at][1]) +
+                                                      S[at][2] * (H[2] - cp.field[at][2]);
+                        }
+                        if (drive_now) {
+#pragma unroll
+                            for (int d = 0; d < 3; ++d) drive_acc(H[d], cp.d1[at][d], cp.d2[at][d], f1, f2);
+                        }
+                        const double kk[3] = {H[1] * S[at][2] - H[2] * S[at][1], H[2] * S[at][0] - H[0] * S[at][2],
+                                              H[0] * S[at][1] - H[1] * S[at][0]};
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            double v;
+                            if (s == 0) {
+                                acc[t][k][at][c] = kk[c];
+                                v = 1.0 * y[t][k][at][c] + (0.5 * dt) * kk[c];
+                            } else if (s == 1) {
+                                acc[t][k][at][c] = acc[t][k][at][c] + 2.0 * kk[c];
+                                v = 1.0 * y[t][k][at][c] + (0.5 * dt) * kk[c];
+                            } else if (s == 2) {
+                                acc[t][k][at][c] = acc[t][k][at][c] + 2.0 * kk[c];
+                                v = 1.0 * y[t][k][at][c] + dt * kk[c];
+                            } else {
+                                y[t][k][at][c] += (dt / 6.0) * (acc[t][k][at][c] + kk[c]);
+                                v = y[t][k][at][c];
+                            }
+                            if (YREG) nx[YREG ? at : 0][c] = v;     // own registers change after the cell
+                            else smem[tout + (at * 3 + c) * G + g] = v;
+                        }
+                    }
+                    if (YREG) {
+#pragma unroll
+                        for (int at = 0; at < NAT; ++at)
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) {
+                                yc[YREG ? t : 0][YREG ? k : 0][at][c] = nx[YREG ? at : 0][c];
+                                smem[tout + (at * 3 + c) * G + g] = nx[YREG ? at : 0][c];
+                            }
+                    }
+                }
+            }
+            if (s == 0 && observe) write_traj(row);
             __syncthreads();
-            if (s == 0 && observe) pending = true;
             const int tmp = in; in = out; out = tmp;
         }
     }
     // Final observation of y(t_end): one more static-field evaluation for E.
     {
-        double part[NV];
 #pragma unroll
         for (int q = 0; q < NV; ++q) part[q] = 0.0;
 #pragma unroll
-        for (int k = 0; k < CPT; ++k) {
-            const int g = tid + k * blockDim.x;
-            if (g >= G) continue;
-            double S[NAT][3];
-            load_cell(in, k, S);
+        for (int t = 0; t < TPC; ++t) {
+            if (t >= ntr) continue;
+            const int tin = t * 2 * SB + in;
 #pragma unroll
-            for (int at = 0; at < NAT; ++at) {
-                double H[3];
-                field_at(in, k, at, S, H);
-                part[3 * at] += S[at][0]; part[3 * at + 1] += S[at][1]; part[3 * at + 2] += S[at][2];
-                part[3 * NAT] += S[at][0] * (H[0] - cp.field[at][0]) + S[at][1] * (H[1] - cp.field[at][1]) +
-                                 S[at][2] * (H[2] - cp.field[at][2]);
+            for (int k = 0; k < CPT; ++k) {
+                const int g = tid + k * blockDim.x;
+                if (g >= G) continue;
+                double S[NAT][3];
+                load_cell(tin, t, k, S);
+#pragma unroll
+                for (int at = 0; at < NAT; ++at) {
+                    double H[3];
+                    field_at(tin, k, at, S, H);
+                    part[t * NR + 3 * at] += S[at][0];
+                    part[t * NR + 3 * at + 1] += S[at][1];
+                    part[t * NR + 3 * at + 2] += S[at][2];
+                    part[t * NR + 3 * NAT] += S[at][0] * (H[0] - cp.field[at][0]) + S[at][1] * (H[1] - cp.field[at][1]) +
+                                              S[at][2] * (H[2] - cp.field[at][2]);
+                }
             }
         }
         write_traj(row);
@@ -419,15 +451,19 @@ rk4_resident_kernel(const __grid_constant__ Couplings<NAT, Z> cp,
         finish_raw(row);
     }
     if (a.y_out) {
-        double* dst = a.y_out + b * (long long)G * NAT * 3;
 #pragma unroll
-        for (int k = 0; k < CPT; ++k) {
-            const int g = tid + k * blockDim.x;
-            if (g >= G) continue;
+        for (int t = 0; t < TPC; ++t) {
+            if (t >= ntr) continue;
+            double* dst = a.y_out + (b0 + t) * (long long)G * NAT * 3;
 #pragma unroll
-            for (int at = 0; at < NAT; ++at)
+            for (int k = 0; k < CPT; ++k) {
+                const int g = tid + k * blockDim.x;
+                if (g >= G) continue;
 #pragma unroll
-                for (int c = 0; c < 3; ++c) dst[((long long)g * NAT + at) * 3 + c] = y[k][at][c];
+                for (int at = 0; at < NAT; ++at)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) dst[((long long)g * NAT + at) * 3 + c] = y[t][k][at][c];
+            }
         }
     }
 }
