@@ -82,6 +82,7 @@ _SIGS = {
     "cmd_batch_rows": (C.c_int64, [C.c_int64, C.c_int64]),
     "cmd_run_batch_device": (C.c_int, [C.c_void_p, C.POINTER(BatchDesc), C.c_void_p, _I32]),
     "cmd_run_batch_device_noalloc": (C.c_int, [C.c_void_p, C.POINTER(BatchDesc), C.c_void_p, _I32]),
+    "cmd_nonlinear_spectrum": (C.c_int, [_D, _D, _D, C.c_int64, C.c_int64, C.c_int32, _D, _D]),
     "cmd_layout_info": (C.c_int, [C.c_void_p, _I64]),
     "cmd_plan_layout": (C.c_int, [C.POINTER(LatticeDesc), _I64]),
     "cmd_run_uneven": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.c_double, C.c_double, C.c_int64]),
@@ -105,6 +106,7 @@ _SIGS = {
     "cmd_lattice_geometry": (C.c_int, [C.c_void_p, _D, _D]),
     "cmd_lattice_desc_of": (C.c_int, [C.c_void_p, C.POINTER(LatticeDesc)]),
     "cmd_lattice_rotate_pulse": (C.c_int, [C.c_void_p, _D, _D, _D]),
+    "cmd_lattice_random_spins": (C.c_int, [C.c_int64, C.c_uint64, C.c_double, _D]),
     "cmd_lattice_free": (None, [C.c_void_p]),
 }
 

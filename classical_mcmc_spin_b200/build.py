@@ -21,7 +21,8 @@ BUILD = PKG / "_build"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-O3"]
-SOURCES = ["cmd_api.cu", "lattice_host.cpp"]
+SOURCES = ["cmd_api.cu", "spectrum.cu", "lattice_host.cpp"]
+DRIVER = PKG / "cmd_spin_solver"          # command-line driver (csrc/spin_solver.cpp) over the C ABI
 
 
 def nvcc() -> str:
@@ -42,6 +43,7 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
     deps = [CSRC / s for s in SOURCES] + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) \
         + list((ROOT / "include").glob("*.h"))
     if not force and not ptxas_info and _newer(LIB, deps):
+        build_driver(verbose, force)
         return LIB
     BUILD.mkdir(exist_ok=True)
     objs = []
@@ -56,12 +58,29 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
         subprocess.run(cmd, check=True)
         objs.append(str(obj))
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart"]
+    cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart", "-lcufft"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
+    build_driver(verbose, True)
     return LIB
+
+
+def build_driver(verbose: bool = False, force: bool = False) -> Path:
+    """The command-line driver, linked against libcmd_b200.so next to it."""
+    deps = [CSRC / "spin_solver.cpp", LIB] + list((ROOT / "include").glob("*.h"))
+    if not force and _newer(DRIVER, deps):
+        return DRIVER
+    cxx = shutil.which("g++") or "g++"
+    tmp = DRIVER.with_suffix(".tmp")
+    cmd = [cxx, "-std=c++17", "-O2", "-I", str(ROOT / "include"), str(CSRC / "spin_solver.cpp"), "-o", str(tmp),
+           "-L", str(PKG), "-lcmd_b200", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, DRIVER)
+    return DRIVER
 
 
 if __name__ == "__main__":

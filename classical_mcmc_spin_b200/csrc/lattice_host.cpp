@@ -353,4 +353,32 @@ int cmd_lattice_rotate_pulse(const cmd_lattice* L, const double* in1, const doub
 
 void cmd_lattice_free(cmd_lattice* L) { delete L; }
 
+// Seeded spins uniform on the sphere of radius spin_length: splitmix64 drives
+// Marsaglia's (1972) rejection method, the method of Lattice::init_random
+// (lattice.h:1115-1124), whose generator the reference seeds from the clock.
+int cmd_lattice_random_spins(int64_t n, uint64_t seed, double spin_length, double* out) {
+    if (n < 0 || (n > 0 && !out) || !(spin_length > 0.0)) return cmd::fail(CMD_ERR_INVALID_ARG, "bad argument");
+    uint64_t state = seed;
+    auto next = [&]() {
+        uint64_t z = (state += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    };
+    auto uniform = [&]() { return (double)(next() >> 11) * (1.0 / 9007199254740992.0); };   // [0, 1)
+    for (int64_t i = 0; i < n; ++i) {
+        double u, v, s;
+        do {
+            u = 2.0 * uniform() - 1.0;
+            v = 2.0 * uniform() - 1.0;
+            s = u * u + v * v;
+        } while (s >= 1.0);
+        const double f = 2.0 * std::sqrt(1.0 - s);
+        out[3 * i] = spin_length * f * u;
+        out[3 * i + 1] = spin_length * f * v;
+        out[3 * i + 2] = spin_length * (1.0 - 2.0 * s);
+    }
+    return CMD_OK;
+}
+
 }  // extern "C"

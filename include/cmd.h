@@ -203,6 +203,20 @@ int cmd_run_batch_device(cmd_handle* h, const cmd_batch_desc* d, void* stream, i
  */
 int cmd_run_batch_device_noalloc(cmd_handle* h, const cmd_batch_desc* d, void* stream, int32_t* launches);
 
+/*
+ * 2DCS analysis step (restates util/readers_new/reader_honeycomb.py:459-553,
+ * which the reference runs offline after pump_probe_spectroscopy).  Inputs are
+ * host arrays of one magnetisation kind (the reader uses M_local): M0 [n_t][3]
+ * (pump only), M1 and M01 [n_tau][n_t][3] (probe only, pump + probe at delay
+ * tau_k).  For component `component`:
+ *   m_nl[k][t]     = M01[k][t] - M0[t] - M1[k][t]
+ *   spectrum[k][t] = | fftshift(fft2(m_nl - mean(m_nl))) | with the omega_t
+ *                    axis flipped, axes (omega_tau, omega_t) as in the reader.
+ * The 2-D FFT runs on the device (cuFFT); either output may be NULL.
+ */
+int cmd_nonlinear_spectrum(const double* M0, const double* M1, const double* M01, int64_t n_tau, int64_t n_t,
+                           int32_t component, double* m_nl, double* spectrum);
+
 /* Lattice layout chosen at cmd_create (for diagnostics and the autotuner):
  * info[0] = sites per group (unit-cell atoms), info[1] = groups,
  * info[2] = max bonds per site kept, info[3] = threads per block of the

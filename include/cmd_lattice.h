@@ -60,6 +60,12 @@ int cmd_lattice_desc_of(const cmd_lattice* L, cmd_lattice_desc* desc);
 int cmd_lattice_rotate_pulse(const cmd_lattice* L, const double* in1, const double* in2,
                              double* field_drive);
 
+/* Seeded initial state (no reference counterpart: Lattice::init_random seeds
+ * from the clock, lattice.h:649): n spins uniform on the sphere of radius
+ * spin_length, Marsaglia's method as in lattice.h:1115-1124, driven by
+ * splitmix64(seed); out [n*3]. */
+int cmd_lattice_random_spins(int64_t n, uint64_t seed, double spin_length, double* out);
+
 void cmd_lattice_free(cmd_lattice* L);
 
 #ifdef __cplusplus

@@ -1,0 +1,155 @@
+"""The command-line driver end to end on the GPU: molecular_dynamics, pump_probe and 2dcs param
+files run through `cmd_spin_solver`, outputs compared with the oracle (rows <= 1e-12, states
+<= 1e-10 as in the parity tests) and the 2DCS spectrum with the oracle's restatement of the
+reference reader (<= 1e-12 of its maximum)."""
+import json
+import subprocess
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL_S = 1e-10
+TOL_M = 1e-12
+
+
+@pytest.fixture(scope="module")
+def driver(native):
+    from classical_mcmc_spin_b200 import build
+    return build.build_driver()
+
+
+def _run(driver, tmp_path, text):
+    p = tmp_path / "run.param"
+    p.write_text(text)
+    r = subprocess.run([str(driver), str(p)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    return r
+
+
+def _state_file(tmp_path, n, seed):
+    from classical_mcmc_spin_b200.states import random_unit_spins
+    s = random_unit_spins(n, seed)
+    path = tmp_path / "init.txt"
+    np.savetxt(path, s, fmt="%.17e")
+    return s.ravel(), path
+
+
+def test_driver_molecular_dynamics(driver, tmp_path, oracle):
+    s0, init = _state_file(tmp_path, 32, 3)
+    out = tmp_path / "md"
+    _run(driver, tmp_path, f"""system = honeycomb_kitaev
+simulation_mode = molecular_dynamics
+lattice_size = 4,4,1
+K = -1.0
+Gamma = 0.25
+Gammap = -0.02
+field_strength = 0.3
+field_direction = 0,1,0
+md_time_start = 0.0
+md_time_end = 1.995
+md_timestep = 0.01
+md_save_interval = 10
+md_integrator = rk4
+initial_spin_config = {init}
+output_dir = {out}
+""")
+    d = out / "sample_0"
+    o = oracle.OracleLattice.kitaev(4, 4, 1, h=0.3, direction=(0, 1, 0))
+    rows, fin = o.md_rk4(s0, 0.0, 1.995, 0.01, 10, gpu_loop=True)
+    t = np.load(d / "trajectory_times.npy")
+    np.testing.assert_array_equal(t, rows[:, 0])
+    for name, cols in (("antiferro", slice(1, 4)), ("local", slice(4, 7)), ("global", slice(7, 10))):
+        m = np.load(d / f"trajectory_magnetization_{name}.npy")
+        assert np.abs(m - rows[:, cols]).max() <= TOL_M
+    assert np.abs(np.load(d / "trajectory_energy_per_site.npy") - rows[:, 10]).max() <= TOL_M
+    spins = np.load(d / "trajectory_spins.npy")
+    np.testing.assert_array_equal(spins[0].ravel(), s0)
+    assert np.abs(spins[-1].ravel() - fin).max() <= TOL_S
+    assert np.abs(np.loadtxt(d / "initial_spins.txt").ravel() - s0).max() == 0.0
+    meta = json.loads((d / "metadata.json").read_text())
+    assert meta["rows"] == len(t) and meta["integration_method"] == "rk4"
+
+
+def test_driver_pump_probe(driver, tmp_path, oracle):
+    s0, init = _state_file(tmp_path, 32, 4)
+    out = tmp_path / "pp"
+    _run(driver, tmp_path, f"""system = honeycomb_kitaev
+simulation_mode = pump_probe
+lattice_size = 4,4,1
+pump_direction = 0,0,1
+pump_amplitude = 0.5
+pump_width = 0.4
+pump_frequency = 0.3
+pump_time = 0.5
+md_time_start = 0.0
+md_time_end = 1.5
+md_timestep = 0.01
+md_integrator = rk4
+initial_spin_config = {init}
+output_dir = {out}
+""")
+    traj = np.loadtxt(out / "sample_0" / "pump_probe_trajectory.txt")
+    o = oracle.OracleLattice.kitaev(4, 4, 1)
+    o.set_pulse(np.tile([0.0, 0.0, 1.0], 2), 0.5, np.zeros(6), 0.0, 0.5, 0.4, 0.3)
+    rows, _ = o.md_rk4(s0, 0.0, 1.5, 0.01, 1, gpu_loop=True)
+    assert traj.shape == (len(rows), 10)
+    np.testing.assert_array_equal(traj[:, 0], rows[:, 0])
+    assert np.abs(traj[:, 1:10] - rows[:, 1:10]).max() <= TOL_M
+
+
+def test_driver_2dcs(driver, tmp_path, oracle):
+    import spectra_oracle as so
+    s0, init = _state_file(tmp_path, 32, 5)
+    out = tmp_path / "2dcs"
+    _run(driver, tmp_path, f"""system = honeycomb_kitaev
+simulation_mode = 2dcs
+lattice_size = 4,4,1
+pump_direction = 0,0,1
+pump_amplitude = 0.4
+pump_width = 0.2
+pump_frequency = 0.5
+tau_start = -0.5
+tau_end = 0.5
+tau_step = 0.25
+md_time_start = -1.0
+md_time_end = 2.0
+md_timestep = 0.01
+md_integrator = rk4
+initial_spin_config = {init}
+output_dir = {out}
+""")
+    d = out / "sample_0"
+    tau = np.load(d / "tau_scan_tau_values.npy")
+    np.testing.assert_allclose(tau, [-0.5, -0.25, 0.0, 0.25, 0.5])
+    times = np.load(d / "reference_times.npy")
+    n_t = len(times)
+    o = oracle.OracleLattice.kitaev(4, 4, 1)
+    z = np.tile([0.0, 0.0, 1.0], 2)
+    B = 1 + 2 * len(tau)
+    t1, t2, s1, s2 = np.zeros(B), np.zeros(B), np.zeros(B), np.zeros(B)
+    s1[0] = 1.0
+    for k, tv in enumerate(tau):
+        t2[1 + 2 * k] = tv
+        s2[1 + 2 * k] = 1.0
+        t2[2 + 2 * k] = tv
+        s1[2 + 2 * k] = s2[2 + 2 * k] = 1.0
+    _, obs = o.batch_rk4(np.tile(s0, (B, 1)), t1, t2, s1, s2, 0.4, 0.2, 0.5, z, z, -1.0, 0.01, n_t - 1)
+    M = {}
+    for q, name in enumerate(("antiferro", "local", "global")):
+        m0 = np.load(d / f"reference_M_{name}.npy")
+        m1 = np.load(d / f"tau_scan_M1_{name}.npy")
+        m01 = np.load(d / f"tau_scan_M01_{name}.npy")
+        assert np.abs(m0 - obs[0, :, 3 * q:3 * q + 3]).max() <= TOL_M
+        assert np.abs(m1 - obs[1::2, :, 3 * q:3 * q + 3]).max() <= TOL_M
+        assert np.abs(m01 - obs[2::2, :, 3 * q:3 * q + 3]).max() <= TOL_M
+        M[name] = (m0, m1, m01)
+    nl = np.load(d / "M_NL_local.npy")
+    sp = np.load(d / "spectrum_local.npy")
+    for c in range(3):
+        np.testing.assert_array_equal(nl[c], so.nonlinear_signal(*M["local"], c))
+        ref = so.compute_2d_fft(so.nonlinear_signal(*M["local"], c))
+        assert np.abs(sp[c] - ref).max() <= 1e-12 * max(1.0, ref.max())
+    meta = json.loads((d / "metadata.json").read_text())
+    assert meta["tau_steps"] == 5 and meta["pulse_amp"] == 0.4
