@@ -106,6 +106,8 @@ struct cmd_handle {
     DevBuf gwork, gmeta, gstat, grows, gqueue;
     DevBuf awork, ackpt, aseg, amloc, aout, ameta, ain;
     DevBuf sbuf, spart, sgpart;  // streamed RK4 / adjoint: stage vectors, tile partials
+    DevBuf chunk_states, chunk_rows;   // cmd_run_batch: ping-pong states and row buffers of time chunks
+    cudaStream_t copy_stream = nullptr;  // cmd_run_batch: device-to-host copies of finished chunks
     bool has_state = false;
     int variant = -1;           // resident-kernel variant; -1 = heuristic default
     // pulse (set_gpu_pulse)
@@ -919,8 +921,9 @@ int cmd_destroy(cmd_handle* h) {
                       &h->pulses, &h->scratch, &h->dframes, &h->dafm, &h->times, &h->drive, &h->raw,
                       &h->tune_states, &h->tune_obs, &h->gwork, &h->gmeta, &h->gstat, &h->grows, &h->gqueue,
                       &h->awork, &h->ackpt, &h->aseg, &h->amloc, &h->aout, &h->ameta, &h->ain,
-                      &h->sbuf, &h->spart, &h->sgpart})
+                      &h->sbuf, &h->spart, &h->sgpart, &h->chunk_states, &h->chunk_rows})
         b->release();
+    if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return CMD_OK;
@@ -1277,6 +1280,83 @@ int run_batch_device(cmd_handle* h, const cmd_batch_desc* d, const cmd::Pulse* d
     return run_rk4(h, r, st, launches);
 }
 
+// Long host-buffer batches run in time chunks so that the observable rows of
+// chunk c travel to the host (second stream) while chunk c+1 computes.  Chunk
+// c starts from chunk c-1's final states at the exact accumulated time of the
+// single-run loop (t += dt from T0), so every step and every row is what one
+// launch would produce; chunk lengths are multiples of save_interval, and a
+// chunk's last row (the next chunk's first) is copied once.
+constexpr int64_t kChunkMinSteps = 4096;
+constexpr int64_t kChunks = 8;
+
+int run_batch_chunked(cmd_handle* h, const cmd_batch_desc* d, const double* d_init, const cmd::Pulse* d_pulses) {
+    const int64_t B = d->B, N3 = h->N * 3, S = d->n_steps, sv = d->save_interval;
+    const int64_t rows_total = rows_for(S, sv);
+    int64_t chunk = (S + kChunks - 1) / kChunks;
+    chunk = (chunk + sv - 1) / sv * sv;
+    const int64_t rows_chunk = rows_for(chunk, sv);
+    if (!h->copy_stream) CUDA_TRY(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+    if (int rc = h->chunk_states.ensure((size_t)2 * B * N3 * sizeof(double))) return rc;
+    if (int rc = h->chunk_rows.ensure((size_t)2 * B * rows_chunk * 10 * sizeof(double))) return rc;
+    double* st[2] = {h->chunk_states.as<double>(), h->chunk_states.as<double>() + B * N3};
+    double* rb[2] = {h->chunk_rows.as<double>(), h->chunk_rows.as<double>() + B * rows_chunk * 10};
+    cudaEvent_t done[2] = {nullptr, nullptr}, copied[2] = {nullptr, nullptr};
+    int rc = CMD_OK;
+    auto cuda_ok = [&](cudaError_t e, const char* what) {
+        if (e == cudaSuccess) return true;
+        rc = fail(CMD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+        return false;
+    };
+    for (int i = 0; i < 2 && rc == CMD_OK; ++i) {
+        cuda_ok(cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming), "cudaEventCreate");
+        if (rc == CMD_OK) cuda_ok(cudaEventCreateWithFlags(&copied[i], cudaEventDisableTiming), "cudaEventCreate");
+    }
+    double t = d->T0;
+    int64_t k0 = 0, c = 0, last = 0;
+    while (rc == CMD_OK && k0 < S) {
+        const int64_t n = std::min(chunk, S - k0);
+        const int slot = (int)(c & 1);
+        const bool final_chunk = k0 + n == S;
+        const int64_t rows_c = rows_for(n, sv);
+        if (c >= 2 && !cuda_ok(cudaStreamWaitEvent(h->stream, copied[slot], 0), "cudaStreamWaitEvent")) break;
+        cmd_batch_desc dd = *d;
+        dd.states = c == 0 ? d_init : st[1 - slot];
+        dd.shared_initial = c == 0 ? d->shared_initial : 0;
+        dd.final_states = st[slot];
+        dd.obs = rb[slot];
+        dd.T0 = t;
+        dd.n_steps = n;
+        if ((rc = run_batch_device(h, &dd, d_pulses, h->stream, nullptr)) != CMD_OK) break;
+        if (!cuda_ok(cudaEventRecord(done[slot], h->stream), "cudaEventRecord")) break;
+        if (!cuda_ok(cudaStreamWaitEvent(h->copy_stream, done[slot], 0), "cudaStreamWaitEvent")) break;
+        const int64_t ncopy = final_chunk ? rows_c : rows_c - 1;
+        if (!cuda_ok(cudaMemcpy2DAsync(d->obs + (k0 / sv) * 10, (size_t)rows_total * 10 * sizeof(double), rb[slot],
+                                       (size_t)rows_c * 10 * sizeof(double), (size_t)ncopy * 10 * sizeof(double),
+                                       (size_t)B, cudaMemcpyDeviceToHost, h->copy_stream),
+                     "cudaMemcpy2DAsync"))
+            break;
+        if (!cuda_ok(cudaEventRecord(copied[slot], h->copy_stream), "cudaEventRecord")) break;
+        for (int64_t k = 0; k < n; ++k) t += d->dt;     // the single-run loop's accumulated time
+        last = slot;
+        k0 += n;
+        ++c;
+    }
+    if (rc == CMD_OK && d->final_states)
+        cuda_ok(cudaMemcpyAsync(d->final_states, st[last], B * N3 * sizeof(double), cudaMemcpyDeviceToHost,
+                                h->stream),
+                "cudaMemcpyAsync");
+    const cudaError_t e1 = cudaStreamSynchronize(h->copy_stream);
+    const cudaError_t e2 = cudaStreamSynchronize(h->stream);
+    for (int i = 0; i < 2; ++i) {
+        if (done[i]) cudaEventDestroy(done[i]);
+        if (copied[i]) cudaEventDestroy(copied[i]);
+    }
+    if (rc != CMD_OK) return rc;
+    if (e1 != cudaSuccess) return fail(CMD_ERR_CUDA, std::string("copy stream: ") + cudaGetErrorString(e1));
+    if (e2 != cudaSuccess) return fail(CMD_ERR_CUDA, std::string("stream: ") + cudaGetErrorString(e2));
+    return CMD_OK;
+}
+
 }  // namespace
 
 int cmd_run_batch(cmd_handle* h, const cmd_batch_desc* d) {
@@ -1290,10 +1370,14 @@ int cmd_run_batch(cmd_handle* h, const cmd_batch_desc* d) {
     const int64_t rows = rows_for(d->n_steps, d->save_interval);
     for (int64_t i = 0; i < n_init * N3; ++i)
         if (!std::isfinite(d->states[i])) return fail(CMD_ERR_NONFINITE, "non-finite initial spin");
-    if (int rc = h->batch_states.ensure((size_t)(n_init + (d->final_states ? B : 0)) * N3 * sizeof(double))) return rc;
-    if (int rc = h->batch_out.ensure((size_t)B * rows * 10 * sizeof(double))) return rc;
+    const bool chunked = d->n_steps >= kChunkMinSteps;
+    if (int rc = h->batch_states.ensure((size_t)(n_init + (d->final_states && !chunked ? B : 0)) * N3 *
+                                        sizeof(double)))
+        return rc;
+    if (!chunked)
+        if (int rc = h->batch_out.ensure((size_t)B * rows * 10 * sizeof(double))) return rc;
     double* d_init = h->batch_states.as<double>();
-    double* d_final = d->final_states ? d_init + n_init * N3 : nullptr;
+    double* d_final = d->final_states && !chunked ? d_init + n_init * N3 : nullptr;
     CUDA_TRY(cudaMemcpyAsync(d_init, d->states, n_init * N3 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     const bool drive = d->d1 || d->d2;
     cmd::Pulse* d_pulses = nullptr;
@@ -1305,6 +1389,7 @@ int cmd_run_batch(cmd_handle* h, const cmd_batch_desc* d) {
         d_pulses = h->pulses.as<cmd::Pulse>();
         CUDA_TRY(cudaMemcpyAsync(d_pulses, hp.data(), B * sizeof(cmd::Pulse), cudaMemcpyHostToDevice, h->stream));
     }
+    if (chunked) return run_batch_chunked(h, d, d_init, d_pulses);
     cmd_batch_desc dd = *d;
     dd.states = d_init;
     dd.obs = h->batch_out.as<double>();
