@@ -12,6 +12,7 @@
 #include "cmd.h"
 #include "cmd_internal.h"
 #include "rk4_resident.cuh"
+#include "rk4_cluster.cuh"
 #include "rk_global.cuh"
 #include "rk_adjoint.cuh"
 #include "rk_stream.cuh"
@@ -107,6 +108,7 @@ struct cmd_handle {
     DevBuf awork, ackpt, aseg, amloc, aout, ameta, ain;
     DevBuf sbuf, spart, sgpart;  // streamed RK4 / adjoint: stage vectors, tile partials
     DevBuf chunk_states, chunk_rows;   // cmd_run_batch: ping-pong states and row buffers of time chunks
+    DevBuf cnbr2, cnbr4;         // partner tables of the 2- and 4-CTA cluster kernels (built at create)
     cudaStream_t copy_stream = nullptr;  // cmd_run_batch: device-to-host copies of finished chunks
     bool has_state = false;
     int variant = -1;           // resident-kernel variant; -1 = heuristic default
@@ -339,6 +341,71 @@ int launch_one(const cmd_handle* h, const cmd::ResidentArgs& args, const double*
     return CMD_OK;
 }
 
+// Partner table of the CS-CTA cluster kernel: the resident table's offsets
+// (atom*3)*G + cell become (rank << 24) | ((atom*3)*Gc + cell - rank*Gc) with
+// Gc = ceil(G / CS) cells per CTA.  Built once per handle.
+int64_t cluster_cells(int64_t G, int cs) { return (G + cs - 1) / cs; }
+
+int upload_cluster_table(cmd_handle* h, int cs) {
+    const Layout& L = h->lay;
+    const int64_t G = L.G, Gc = cluster_cells(G, cs);
+    if ((int64_t)L.NA * 3 * Gc >= (1 << cmd::kClusterRankShift)) return CMD_OK;   // never launched
+    std::vector<int> t(L.nbr.size(), 0);
+    for (size_t i = 0; i < L.nbr.size(); ++i) {
+        const int64_t off = L.nbr[i];
+        const int64_t at = off / (3 * G), c = off - at * 3 * G;     // partner atom*3 block and cell
+        const int64_t gp = c % G, comp = c / G;                     // comp is 0 for the offsets stored
+        const int64_t r = gp / Gc, l = gp - r * Gc;
+        t[i] = (int)((r << cmd::kClusterRankShift) | ((at * 3 + comp) * Gc + l));
+    }
+    DevBuf& d = cs == 2 ? h->cnbr2 : h->cnbr4;
+    if (int rc = d.ensure(std::max<size_t>(t.size(), 1) * sizeof(int))) return rc;
+    if (!t.empty() && cudaMemcpy(d.p, t.data(), t.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(CMD_ERR_CUDA, "cluster neighbour table upload failed");
+    return CMD_OK;
+}
+
+size_t cluster_smem(int NA, int64_t G, int cs) {
+    return ((size_t)2 * NA * 3 * cluster_cells(G, cs) + 32 * cmd::kRedStride + 12 + 16) * sizeof(double);
+}
+
+template <int NAT, int Z, int LZ, int CS, int MAXT>
+int launch_cluster(const cmd_handle* h, const cmd::ResidentArgs& args, const double* d1, const double* d2,
+                   int64_t B, cudaStream_t st) {
+    auto kern = cmd::rk4_cluster_kernel<NAT, Z, LZ, CS, MAXT>;
+    const int64_t G = h->lay.G, Gc = cluster_cells(G, CS);
+    const int threads = (int)((Gc + 31) / 32 * 32);
+    if (threads > MAXT) return fail(CMD_ERR_UNSUPPORTED, "lattice too large for this cluster variant");
+    const size_t smem = cluster_smem(NAT, G, CS);
+    if (smem > kMaxSmem) return fail(CMD_ERR_UNSUPPORTED, "stage buffers exceed shared memory");
+    const DevBuf& tab = CS == 2 ? h->cnbr2 : h->cnbr4;
+    if (!tab.p) return fail(CMD_ERR_UNSUPPORTED, "no cluster neighbour table for this lattice");
+    static bool attr_set = false;
+    if (!attr_set) {
+        CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
+        attr_set = true;
+    }
+    cmd::Couplings<NAT, Z> cp;
+    fill_couplings<NAT, Z>(h, d1, d2, cp);
+    cmd::ResidentArgs a = args;
+    a.B = B;
+    a.nbr = static_cast<const int*>(tab.p);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(B * CS));
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CS;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, cp, a, (int)Gc));
+    return CMD_OK;
+}
+
 // Resident-kernel variants compiled into the library: (atoms/cell, bonds/atom,
 // in-cell bonds) x (cells per thread, max threads, min CTAs per SM, own stage
 // input kept in registers, trajectories per CTA).  The autotuner times the
@@ -347,14 +414,18 @@ struct Variant {
     int NAT, Z, LZ, CPT, MAXT, MINB;
     bool YREG;
     int TPC;
+    int CS;                       // CTAs per trajectory (thread-block cluster), 1 = one CTA
     LaunchFn fn;
     const char* name;
 };
 
 #define CMD_VARIANT(NAT, Z, LZ, CPT, MAXT, MINB, YREG, TPC) \
-    Variant{NAT, Z, LZ, CPT, MAXT, MINB, YREG, TPC, &launch_one<NAT, Z, LZ, CPT, MAXT, MINB, YREG, TPC>, \
+    Variant{NAT, Z, LZ, CPT, MAXT, MINB, YREG, TPC, 1, &launch_one<NAT, Z, LZ, CPT, MAXT, MINB, YREG, TPC>, \
             "rk4_resident<" #NAT "," #Z "," #LZ "> cpt=" #CPT " maxt=" #MAXT " minb=" #MINB " yreg=" #YREG \
             " tpc=" #TPC}
+#define CMD_CLUSTER(NAT, Z, LZ, CS, MAXT) \
+    Variant{NAT, Z, LZ, 1, MAXT, 1, true, 1, CS, &launch_cluster<NAT, Z, LZ, CS, MAXT>, \
+            "rk4_cluster<" #NAT "," #Z "," #LZ "> cs=" #CS " maxt=" #MAXT}
 
 const Variant kVariants[] = {
     // 2-atom cells with 3 bonds per site (Kitaev / Heisenberg honeycomb)
@@ -370,15 +441,25 @@ const Variant kVariants[] = {
     CMD_VARIANT(2, 3, 1, 1, 640, 1, false, 2),
     CMD_VARIANT(2, 3, 1, 1, 640, 1, true, 2),
     CMD_VARIANT(2, 3, 1, 2, 320, 1, false, 2),
+    // one trajectory over a cluster of 2 or 4 CTAs (distributed shared memory)
+    CMD_CLUSTER(2, 3, 1, 2, 640),
+    CMD_CLUSTER(2, 3, 1, 4, 640),
     // 4-atom cells with 6 bonds per site (nearest-neighbour pyrochlore)
     CMD_VARIANT(4, 6, 3, 1, 512, 1, true, 1),
     CMD_VARIANT(4, 6, 3, 2, 256, 2, false, 1),
     CMD_VARIANT(4, 6, 3, 2, 512, 1, false, 1),
+    CMD_CLUSTER(4, 6, 3, 2, 512),
+    CMD_CLUSTER(4, 6, 3, 4, 512),
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 
 bool variant_fits(const Variant& v, const Layout& L) {
     if (!L.uniform || v.NAT != L.NA || v.Z != L.Z || v.LZ != L.LZ) return false;
+    if (v.CS > 1) {
+        const int64_t Gc = cluster_cells(L.G, v.CS);
+        return Gc >= 32 && (Gc + 31) / 32 * 32 <= v.MAXT && cluster_smem(v.NAT, L.G, v.CS) <= kMaxSmem &&
+               (int64_t)v.NAT * 3 * Gc < (1 << cmd::kClusterRankShift);
+    }
     const int64_t threads = ((L.G + v.CPT - 1) / v.CPT + 31) / 32 * 32;
     if (threads > v.MAXT) return false;
     const size_t smem = resident_smem(v.NAT, L.G, v.TPC);
@@ -903,6 +984,8 @@ int cmd_create(const cmd_lattice_desc* d, cmd_handle** out) {
         if (rc == CMD_OK && !h->lay.nbr.empty() &&
             cudaMemcpy(h->nbr.p, h->lay.nbr.data(), h->lay.nbr.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
             rc = fail(CMD_ERR_CUDA, "neighbour table upload failed");
+        for (int cs : {2, 4})
+            if (rc == CMD_OK) rc = upload_cluster_table(h, cs);
     }
     if (rc == CMD_OK) rc = h->state.ensure((size_t)h->N * 3 * sizeof(double));
     if (rc == CMD_OK) rc = upload_frames(h, h->frames.data(), h->afm.data());
@@ -921,7 +1004,7 @@ int cmd_destroy(cmd_handle* h) {
                       &h->pulses, &h->scratch, &h->dframes, &h->dafm, &h->times, &h->drive, &h->raw,
                       &h->tune_states, &h->tune_obs, &h->gwork, &h->gmeta, &h->gstat, &h->grows, &h->gqueue,
                       &h->awork, &h->ackpt, &h->aseg, &h->amloc, &h->aout, &h->ameta, &h->ain,
-                      &h->sbuf, &h->spart, &h->sgpart, &h->chunk_states, &h->chunk_rows})
+                      &h->sbuf, &h->spart, &h->sgpart, &h->chunk_states, &h->chunk_rows, &h->cnbr2, &h->cnbr4})
         b->release();
     if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
     if (h->stream) cudaStreamDestroy(h->stream);

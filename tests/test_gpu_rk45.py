@@ -95,7 +95,7 @@ def test_dopri5_fixed_matches_reference_gpu(api, oracle):
 
 
 def test_streamed_rk4_for_large_lattice(api, oracle):
-    """48x48 honeycomb (4608 spins) does not fit the resident kernel: RK4 runs as streamed stage kernels."""
+    """48x48 honeycomb (4608 spins) does not fit one CTA: RK4 runs on a 4-CTA cluster."""
     lat, o = _kitaev(oracle, 48, 48)
     s0 = _spins(lat.lattice_size, 34)
     h = lat.to_gpu()

@@ -1,4 +1,5 @@
-"""Streamed RK4 and adjoint (rk_stream.cuh): lattices no resident CTA holds.
+"""RK4 and adjoint on lattices one CTA cannot hold: streamed stages (rk_stream.cuh) and, where a
+thread-block cluster holds the lattice, the cluster kernel (rk4_cluster.cuh).
 
 Each RK4 stage is one launch over (cell tile, trajectory).  Same tolerances as
 the resident path: states <= 1e-10, magnetisations / energy rows <= 1e-12
@@ -30,13 +31,22 @@ def _streamed(h):
     return all(not fits for _, _, fits in h.variants())
 
 
-def test_streamed_batch_pump_probe_matches_oracle(api, oracle):
-    """Kitaev 48x48 (4608 spins), per-trajectory pulse pairs, streamed stages."""
+def _default(h):
+    """The variant a handle uses by default: the first that fits."""
+    return next(i for i, _, fits in h.variants() if fits)
+
+
+@pytest.mark.parametrize("L,streamed", [(64, True), (48, False)])
+def test_batch_pump_probe_matches_oracle(api, oracle, L, streamed):
+    """Per-trajectory pulse pairs on lattices one CTA cannot hold: Kitaev 64x64 (8192 spins, streamed
+    stages) and 48x48 (4608 spins, one trajectory per 4-CTA cluster)."""
     from classical_mcmc_spin_b200.lattice import Lattice
-    lat = Lattice.kitaev(48, 48, 1)
-    o = oracle.OracleLattice.kitaev(48, 48, 1)
+    lat = Lattice.kitaev(L, L, 1)
+    o = oracle.OracleLattice.kitaev(L, L, 1)
     h = lat.to_gpu()
-    assert _streamed(h)
+    assert _streamed(h) == streamed
+    if not streamed:
+        assert h.variants()[h.get_variant() if h.get_variant() >= 0 else _default(h)][1].startswith("rk4_cluster")
     s0 = _spins(lat.lattice_size, 21)
     fin = np.tile(R111, 2)
     fd = lat.rotate_pulse(fin, fin)
@@ -60,14 +70,16 @@ def oracle_batch(o, states, t1, t2, a1, a2, fin, nsteps):
                        nsteps)
 
 
-def test_streamed_pyrochlore_integrate_with_states(api, oracle):
-    """Pyrochlore 8^3 conventional cells (8192 spins) with a [111] field: rows, saved states, final state."""
+@pytest.mark.parametrize("L,streamed", [(10, True), (8, False)])
+def test_pyrochlore_integrate_with_states(api, oracle, L, streamed):
+    """Pyrochlore with a [111] field on 10^3 conventional cells (16000 spins, streamed) and 8^3 cells
+    (8192 spins, 4-CTA cluster): rows, saved states, final state."""
     from classical_mcmc_spin_b200.lattice import Lattice
     kw = dict(h=0.2, Jzz=1.0, Jpm=0.05, Jpmpm=0.02)
-    lat = Lattice.pyrochlore_non_kramer(8, 8, 8, field_direction=R111, cubic=True, **kw)
-    o = oracle.OracleLattice.pyrochlore_nk(8, 8, 8, direction=R111, cubic=True, **kw)
+    lat = Lattice.pyrochlore_non_kramer(L, L, L, field_direction=R111, cubic=True, **kw)
+    o = oracle.OracleLattice.pyrochlore_nk(L, L, L, direction=R111, cubic=True, **kw)
     h = lat.to_gpu()
-    assert _streamed(h)
+    assert _streamed(h) == streamed
     s0 = _spins(lat.lattice_size, 22)
     api.set_gpu_spins(h, s0)
     traj, obs, times = api.integrate_gpu(h, 0.0, 0.4975, 0.005, 10, "rk4", with_states=True)
