@@ -240,19 +240,12 @@ def leg_adjoint_kitaev(torch, dev, S=20000):
     return out
 
 
-def leg_pyrochlore(torch, dev, S=20000, S_adj=2000):
-    """Large pyrochlore: 16^3 conventional cells (65536 spins), Jzz=1, J+-=0.05, J+-+-=0.02, h=0.2 along [111],
-    32 states (seed 5), RK4 dt 0.005.  Forward through cmd_run_batch_device (device buffers, CUDA events, M and E
-    every step); adjoint w.r.t. (Jzz, J+-, J+-+-, h) against targets at (1, 0.06, 0.03, 0.25)."""
+def _forward_device(torch, dev, h, states, S, dt, streamed):
+    """B trajectories from `states` for S RK4 steps through cmd_run_batch_device (device buffers, no drive,
+    M and E every step), timed with CUDA events on the launching stream."""
     from classical_mcmc_spin_b200 import _native as nat
-    from classical_mcmc_spin_b200 import adjoint as A
-    from classical_mcmc_spin_b200.states import random_unit_spins
-    theta = np.array([1.0, 0.05, 0.02, 0.2])
-    build = lambda th: A.pyrochlore_lattice(th, 16, 16, 16, cubic=True)
-    lat = build(theta)
-    N, B, dt = lat.lattice_size, 32, 0.005
-    h = lat.to_gpu()
-    states = np.stack([random_unit_spins(N, 5000 + b).ravel() for b in range(B)])
+    B, N3 = states.shape
+    N = N3 // 3
     d_states = torch.from_numpy(states).to(dev).contiguous()
     rows = int(nat.lib().cmd_batch_rows(S, 1))
     d_obs = torch.empty((B, rows, 10), dtype=torch.float64, device=dev)
@@ -283,12 +276,43 @@ def leg_pyrochlore(torch, dev, S=20000, S_adj=2000):
     torch.cuda.synchronize(dev)
     ms = e0.elapsed_time(e1)
     value = B * N * S / (ms * 1e-3)
-    norm_dev = float((d_fin.view(B, N, 3).norm(dim=2) - 1).abs().max().item())
-    fwd = {"value": value, "unit": UNIT, "ms": ms, "rk4_steps": S, "launches": launches.value,
-           "hbm_bytes_per_spin_step": STREAM_BYTES_PER_SPIN_STEP,
-           "achieved_gbs": STREAM_BYTES_PER_SPIN_STEP * value / 1e9,
-           "final_norm_dev_max": norm_dev, "observables_finite": bool(torch.isfinite(d_obs).all().item())}
-    del d_obs, d_fin, d_states
+    out = {"value": value, "unit": UNIT, "ms": ms, "rk4_steps": S, "launches": launches.value,
+           "final_norm_dev_max": float((d_fin.view(B, N, 3).norm(dim=2) - 1).abs().max().item()),
+           "observables_finite": bool(torch.isfinite(d_obs).all().item())}
+    if streamed:
+        out["hbm_bytes_per_spin_step"] = STREAM_BYTES_PER_SPIN_STEP
+        out["achieved_gbs"] = STREAM_BYTES_PER_SPIN_STEP * value / 1e9
+    return out
+
+
+def leg_kitaev48_forward(torch, dev, S=20000):
+    """Forward of the adjoint workload: honeycomb 48x48 (4608 spins), 64 states (seed 4), RK4 dt 0.01, one
+    trajectory per 4-CTA cluster (the lattice does not fit one CTA)."""
+    from classical_mcmc_spin_b200 import adjoint as A
+    from classical_mcmc_spin_b200.states import random_unit_spins
+    lat = A.kitaev_lattice(np.array([-1.0, 0.25, -0.02, 0.0, 0.0]), 48, 48)
+    h = lat.to_gpu()
+    states = np.stack([random_unit_spins(lat.lattice_size, 4000 + b).ravel() for b in range(64)])
+    out = _forward_device(torch, dev, h, states, S, 0.01, streamed=False)
+    out["variant"] = next(n for i, n, _ in h.variants() if i == h.get_variant())
+    out["workload"] = "kitaev48x48_64traj_rk4_forward"
+    h.close()
+    return out
+
+
+def leg_pyrochlore(torch, dev, S=20000, S_adj=2000):
+    """Large pyrochlore: 16^3 conventional cells (65536 spins), Jzz=1, J+-=0.05, J+-+-=0.02, h=0.2 along [111],
+    32 states (seed 5), RK4 dt 0.005.  Forward through cmd_run_batch_device (device buffers, CUDA events, M and E
+    every step); adjoint w.r.t. (Jzz, J+-, J+-+-, h) against targets at (1, 0.06, 0.03, 0.25)."""
+    from classical_mcmc_spin_b200 import adjoint as A
+    from classical_mcmc_spin_b200.states import random_unit_spins
+    theta = np.array([1.0, 0.05, 0.02, 0.2])
+    build = lambda th: A.pyrochlore_lattice(th, 16, 16, 16, cubic=True)
+    lat = build(theta)
+    N, B, dt = lat.lattice_size, 32, 0.005
+    h = lat.to_gpu()
+    states = np.stack([random_unit_spins(N, 5000 + b).ravel() for b in range(B)])
+    fwd = _forward_device(torch, dev, h, states, S, dt, streamed=True)
     h.close()
     adj = _adjoint_leg(torch, dev, build, theta, np.array([1.0, 0.06, 0.03, 0.25]), 4, B, S_adj, dt, 5,
                        int(np.ceil(np.sqrt(S_adj))))
@@ -370,7 +394,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
     ap.add_argument("--no-peak", action="store_true", help="skip the DGEMM peak probe (profiling runs)")
-    ap.add_argument("--legs", default="uneven,adjoint,pyrochlore",
+    ap.add_argument("--legs", default="uneven,adjoint,kitaev48,pyrochlore",
                     help="further workloads to time on rank 0 (comma list; empty for none)")
     ap.add_argument("--adjoint-steps", type=int, default=20000, help="RK4 steps of the 48x48 adjoint leg")
     ap.add_argument("--pyro-steps", type=int, default=20000, help="RK4 steps of the 65536-spin forward leg")
@@ -553,6 +577,8 @@ def main():
             legs["uneven_rk45"] = leg_uneven(torch, dev)
         if "adjoint" in want:
             legs["adjoint_kitaev48"] = leg_adjoint_kitaev(torch, dev, S=args.adjoint_steps)
+        if "kitaev48" in want:
+            legs["kitaev48_forward"] = leg_kitaev48_forward(torch, dev)
         if "pyrochlore" in want:
             legs["pyrochlore65536"] = leg_pyrochlore(torch, dev, S=args.pyro_steps, S_adj=args.pyro_adjoint_steps)
 
