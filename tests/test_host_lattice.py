@@ -85,8 +85,10 @@ def test_layout_plan_pyrochlore_drops_zero_j2(native):
 def test_layout_plan_rejects_with_reason(native):
     rc, info, msg = _plan(Lattice.kitaev(8, 8, 1, J2_A=0.1, J2_B=0.1))
     assert rc == nat.CMD_ERR_UNSUPPORTED and "9 bonds/site" in msg
-    rc, info, msg = _plan(Lattice.kitaev(48, 48, 1))
-    assert rc == nat.CMD_ERR_UNSUPPORTED and "2304 cells" in msg
+    rc, info, msg = _plan(Lattice.kitaev(64, 64, 1))         # no CTA or 4-CTA cluster holds 4096 cells
+    assert rc == nat.CMD_ERR_UNSUPPORTED and "4096 cells" in msg
+    rc, info, _ = _plan(Lattice.kitaev(48, 48, 1))           # 4 CTAs of 576 cells
+    assert rc == nat.CMD_OK and info[3] == 576 and info[5] == (2 * 576 * 2 * 3 + 32 * 16 + 12 + 16) * 8
 
 
 def test_layout_plan_rejects_non_uniform_couplings(native):
