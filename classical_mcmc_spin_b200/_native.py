@@ -25,6 +25,7 @@ CMD_ERR_STATE = 7
 CMD_RK4 = 0
 CMD_DOPRI5_FIXED = 1
 CMD_RK45 = 2
+CMD_CASH_KARP_FIXED = 3
 
 STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "UNSUPPORTED", 3: "CUDA_ERROR", 4: "NONFINITE",
                 5: "WATCHDOG_TIMEOUT", 6: "OOM", 7: "STATE"}

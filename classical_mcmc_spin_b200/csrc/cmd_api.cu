@@ -1105,7 +1105,10 @@ int run_single(cmd_handle* h, double T0, double dt, int64_t n_steps, int64_t sav
 namespace {
 
 int mode_of(int method) {
-    return method == CMD_RK45 ? cmd::kModeRK45 : (method == CMD_DOPRI5_FIXED ? cmd::kModeDopri5Fixed : cmd::kModeRK4);
+    return method == CMD_RK45               ? cmd::kModeRK45
+           : method == CMD_DOPRI5_FIXED     ? cmd::kModeDopri5Fixed
+           : method == CMD_CASH_KARP_FIXED ? cmd::kModeCashKarpFixed
+                                            : cmd::kModeRK4;
 }
 
 // One trajectory of the handle through the global-state integrator.
@@ -1142,8 +1145,9 @@ bool rk4_fits(const cmd_handle* h) { return resident_fits(h) || global_type(h->l
 int cmd_step(cmd_handle* h, double t, double dt, int method) {
     cmd::clear_error();
     if (int rc = check_handle(h, true)) return rc;
-    if (method != CMD_RK4 && method != CMD_DOPRI5_FIXED)
-        return fail(CMD_ERR_INVALID_ARG, "cmd_step takes a fixed-step method (CMD_RK4 or CMD_DOPRI5_FIXED)");
+    if (method != CMD_RK4 && method != CMD_DOPRI5_FIXED && method != CMD_CASH_KARP_FIXED)
+        return fail(CMD_ERR_INVALID_ARG,
+                    "cmd_step takes a fixed-step method (CMD_RK4, CMD_DOPRI5_FIXED or CMD_CASH_KARP_FIXED)");
     if (!std::isfinite(t) || !std::isfinite(dt)) return fail(CMD_ERR_INVALID_ARG, "non-finite t or dt");
     if (method == CMD_RK4 && resident_fits(h)) return run_single(h, t, dt, 1, 1, (double)h->N, false, false, true);
     return run_global_single(h, method, t, t + dt, dt, 1, 1, 0, false, nullptr);
@@ -1153,7 +1157,7 @@ int cmd_integrate(cmd_handle* h, double T0, double T1, double dt, int64_t save_i
                   double* times, double* obs, double* states, int64_t max_rows, int64_t* rows_out) {
     cmd::clear_error();
     if (int rc = check_handle(h, true)) return rc;
-    if (method != CMD_RK4 && method != CMD_DOPRI5_FIXED && method != CMD_RK45)
+    if (method != CMD_RK4 && method != CMD_DOPRI5_FIXED && method != CMD_RK45 && method != CMD_CASH_KARP_FIXED)
         return fail(CMD_ERR_INVALID_ARG, "unknown integration method");
     if (save_interval <= 0 || !(dt > 0.0) || !std::isfinite(T0) || !std::isfinite(T1))
         return fail(CMD_ERR_INVALID_ARG, "bad integration window");
@@ -1209,7 +1213,7 @@ int cmd_run_uneven(cmd_traj_spec* specs, int64_t B, int method, double abs_tol, 
                    int64_t max_steps) {
     cmd::clear_error();
     if (!specs || B <= 0) return fail(CMD_ERR_INVALID_ARG, "empty batch");
-    if (method != CMD_RK4 && method != CMD_DOPRI5_FIXED && method != CMD_RK45)
+    if (method != CMD_RK4 && method != CMD_DOPRI5_FIXED && method != CMD_RK45 && method != CMD_CASH_KARP_FIXED)
         return fail(CMD_ERR_INVALID_ARG, "unknown integration method");
     if (method == CMD_RK45 && (!(abs_tol >= 0.0) || !(rel_tol >= 0.0) || (abs_tol == 0.0 && rel_tol == 0.0)))
         return fail(CMD_ERR_INVALID_ARG, "bad tolerances");
@@ -1678,6 +1682,17 @@ int stream_adjoint(cmd_handle* h, const StreamAdjJob& j, const std::vector<doubl
     return CMD_OK;
 }
 
+// Threads per CTA and shared memory per CTA of variant V on layout L.
+void variant_shape(const Variant& V, const Layout& L, int64_t* threads, int64_t* smem) {
+    if (V.CS > 1) {
+        *threads = (cluster_cells(L.G, V.CS) + 31) / 32 * 32;
+        *smem = (int64_t)cluster_smem(L.NA, L.G, V.CS);
+    } else {
+        *threads = ((L.G + V.CPT - 1) / V.CPT + 31) / 32 * 32;
+        *smem = (int64_t)resident_smem(L.NA, L.G, V.TPC);
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -1816,9 +1831,8 @@ int cmd_plan_layout(const cmd_lattice_desc* d, int64_t* info) {
     const int vi = default_variant(L);
     if (vi < 0) return no_instance(L);
     const Variant& V = kVariants[vi];
-    info[3] = ((L.G + V.CPT - 1) / V.CPT + 31) / 32 * 32;
+    variant_shape(V, L, &info[3], &info[5]);
     info[4] = V.CPT;
-    info[5] = (int64_t)resident_smem(L.NA, L.G);
     return CMD_OK;
 }
 
@@ -1833,9 +1847,8 @@ int cmd_layout_info(cmd_handle* h, int64_t* info) {
     const int vi = pick_variant(h);
     if (vi < 0) return no_instance(h->lay);
     const Variant& V = kVariants[vi];
-    info[3] = ((h->lay.G + V.CPT - 1) / V.CPT + 31) / 32 * 32;
+    variant_shape(V, h->lay, &info[3], &info[5]);
     info[4] = V.CPT;
-    info[5] = (int64_t)resident_smem(h->lay.NA, h->lay.G);
     return CMD_OK;
 }
 

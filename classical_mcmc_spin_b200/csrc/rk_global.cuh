@@ -27,7 +27,7 @@
 
 namespace cmd {
 
-enum { kModeRK45 = 0, kModeDopri5Fixed = 1, kModeRK4 = 2 };
+enum { kModeRK45 = 0, kModeDopri5Fixed = 1, kModeRK4 = 2, kModeCashKarpFixed = 3 };
 
 constexpr int kGVectors = 12;   // y, ynew, Ya, Yb, k1..k7, spare
 
@@ -342,17 +342,25 @@ __device__ void run_trajectory(const Couplings<NAT, Z>& cp, const GTraj& T, cons
         }
     } else {
         // Fixed-step modes follow the reference GPU loop: rows every save_every
-        // steps from the k1 evaluation, plus a final observation.
-        static constexpr double a21 = 1.0 / 5.0;
-        static constexpr double a31 = 3.0 / 40.0, a32 = 9.0 / 40.0;
-        static constexpr double a41 = 44.0 / 45.0, a42 = -56.0 / 15.0, a43 = 32.0 / 9.0;
-        static constexpr double a51 = 19372.0 / 6561.0, a52 = -25360.0 / 2187.0, a53 = 64448.0 / 6561.0,
-                                a54 = -212.0 / 729.0;
-        static constexpr double a61 = 9017.0 / 3168.0, a62 = -355.0 / 33.0, a63 = 46732.0 / 5247.0,
-                                a64 = 49.0 / 176.0, a65 = -5103.0 / 18656.0;
-        static constexpr double c2 = 1.0 / 5.0, c3 = 3.0 / 10.0, c4 = 4.0 / 5.0, c5 = 8.0 / 9.0;
-        static constexpr double b1 = 35.0 / 384.0, b3 = 500.0 / 1113.0, b4 = 125.0 / 192.0,
-                                b5 = -2187.0 / 6784.0, b6 = 11.0 / 84.0;
+        // steps from the k1 evaluation, plus a final observation.  The six-stage
+        // tableaux: Dormand-Prince 5 (integrator.cuh:186-228) and Cash-Karp 5
+        // (integrator.cuh:141-185, "rk5"), whose final update the reference
+        // forms with the dopri5 kernel, b5 = 0 and k6 in the k5 slot.
+        const bool ck = a.mode == kModeCashKarpFixed;
+        const double a21 = 1.0 / 5.0, a31 = 3.0 / 40.0, a32 = 9.0 / 40.0;
+        const double a41 = ck ? 3.0 / 10.0 : 44.0 / 45.0, a42 = ck ? -9.0 / 10.0 : -56.0 / 15.0;
+        const double a43 = ck ? 6.0 / 5.0 : 32.0 / 9.0;
+        const double a51 = ck ? -11.0 / 54.0 : 19372.0 / 6561.0, a52 = ck ? 5.0 / 2.0 : -25360.0 / 2187.0;
+        const double a53 = ck ? -70.0 / 27.0 : 64448.0 / 6561.0, a54 = ck ? 35.0 / 27.0 : -212.0 / 729.0;
+        const double a61 = ck ? 1631.0 / 55296.0 : 9017.0 / 3168.0, a62 = ck ? 175.0 / 512.0 : -355.0 / 33.0;
+        const double a63 = ck ? 575.0 / 13824.0 : 46732.0 / 5247.0, a64 = ck ? 44275.0 / 110592.0 : 49.0 / 176.0;
+        const double a65 = ck ? 253.0 / 4096.0 : -5103.0 / 18656.0;
+        const double c2 = 1.0 / 5.0, c3 = 3.0 / 10.0, c4 = ck ? 3.0 / 5.0 : 4.0 / 5.0, c5 = ck ? 1.0 : 8.0 / 9.0;
+        const double c6 = ck ? 7.0 / 8.0 : 1.0;
+        const double b1 = ck ? 37.0 / 378.0 : 35.0 / 384.0, b3 = ck ? 250.0 / 621.0 : 500.0 / 1113.0;
+        const double b4 = ck ? 125.0 / 594.0 : 125.0 / 192.0, b5 = ck ? 0.0 : -2187.0 / 6784.0;
+        const double b6 = ck ? 512.0 / 1771.0 : 11.0 / 84.0;
+        double* const k5b = ck ? k[5] : k[4];       // the reference's k5 slot (k6 again for Cash-Karp)
         const double dt = T.dt0;
         long long save_left = 0;
         for (long long step = 0; step < T.n_steps; ++step) {
@@ -389,7 +397,7 @@ __device__ void run_trajectory(const Couplings<NAT, Z>& cp, const GTraj& T, cons
                         y[i] += (dt / 6.0) * (k[0][i] + 2.0 * k[1][i] + 2.0 * k[2][i] + k[3][i]);
                     }
                 __syncthreads();
-            } else {                            // integrator.cuh:186-228 arithmetic
+            } else {                            // integrator.cuh:141-228 arithmetic
                 __syncthreads();
                 for (int g = tid; g < G; g += nt)
                     for (int e = 0; e < NAT * 3; ++e) {
@@ -426,11 +434,11 @@ __device__ void run_trajectory(const Couplings<NAT, Z>& cp, const GTraj& T, cons
                                              a65 * k[4][i]);
                     }
                 __syncthreads();
-                rhs(Ya, k[5], t + dt, nullptr);
+                rhs(Ya, k[5], t + c6 * dt, nullptr);
                 for (int g = tid; g < G; g += nt)
                     for (int e = 0; e < NAT * 3; ++e) {
                         const long long i = (long long)e * G + g;
-                        y[i] += dt * (b1 * k[0][i] + b3 * k[2][i] + b4 * k[3][i] + b5 * k[4][i] + b6 * k[5][i]);
+                        y[i] += dt * (b1 * k[0][i] + b3 * k[2][i] + b4 * k[3][i] + b5 * k5b[i] + b6 * k[5][i]);
                     }
                 __syncthreads();
             }
@@ -456,7 +464,7 @@ __device__ void run_trajectory(const Couplings<NAT, Z>& cp, const GTraj& T, cons
 }
 
 template <int NA0, int Z0, int LZ0, int NA1, int Z1, int LZ1>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 1)
 rk_global_kernel(const __grid_constant__ Couplings<NA0, Z0> c0, const __grid_constant__ Couplings<NA1, Z1> c1,
                  const __grid_constant__ GArgs a) {
     __shared__ double sh[32 * kRedStride + 16 + 32];

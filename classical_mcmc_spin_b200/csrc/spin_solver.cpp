@@ -215,9 +215,10 @@ Config parse_file(const std::string& path) {
     if (!(c.md_timestep > 0.0)) throw ConfigError("md_timestep must be positive");
     if (c.md_save_interval < 1) throw ConfigError("md_save_interval must be >= 1");
     if (c.num_trials < 1) throw ConfigError("num_trials must be >= 1");
-    if (c.mode != "2dcs" && c.md_integrator != "rk4" && c.md_integrator != "dopri5")
-        throw ConfigError("md_integrator '" + c.md_integrator + "' is not on this path (rk4, dopri5; set md_adaptive = "
-                          "true for dopri5 with step control)");
+    if (c.mode != "2dcs" && c.md_integrator != "rk4" && c.md_integrator != "dopri5" && c.md_integrator != "rk5" &&
+        c.md_integrator != "rkck54")
+        throw ConfigError("md_integrator '" + c.md_integrator + "' is not on this path (rk4, rk5, dopri5; set "
+                          "md_adaptive = true for dopri5 with step control)");
     for (int i = 0; i < 3; ++i)
         if (c.L[i] < 1) throw ConfigError("lattice_size entries must be >= 1");
     return c;
@@ -351,8 +352,9 @@ int method_of(const Config& c) {
     const std::string& m = c.md_integrator;
     if (m == "rk4") return CMD_RK4;
     if (m == "dopri5") return c.md_adaptive ? CMD_RK45 : CMD_DOPRI5_FIXED;
-    throw ConfigError("md_integrator '" + m + "' is not on this path (rk4, dopri5; set md_adaptive = true for "
-                      "dopri5 with step control)");
+    if (m == "rk5" || m == "rkck54") return CMD_CASH_KARP_FIXED;
+    throw ConfigError("md_integrator '" + m + "' is not on this path (rk4, rk5, dopri5; set md_adaptive = true "
+                      "for dopri5 with step control)");
 }
 
 struct Rows {

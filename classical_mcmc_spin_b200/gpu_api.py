@@ -18,7 +18,8 @@ import numpy as np
 from . import _native as nat
 from ._native import check, dptr, f64, iptr
 
-METHODS = {"rk4": nat.CMD_RK4, "dopri5": nat.CMD_DOPRI5_FIXED, "rk45": nat.CMD_RK45}
+METHODS = {"rk4": nat.CMD_RK4, "dopri5": nat.CMD_DOPRI5_FIXED, "rk45": nat.CMD_RK45,
+           "rk5": nat.CMD_CASH_KARP_FIXED, "rkck54": nat.CMD_CASH_KARP_FIXED}
 
 
 def _method(method: str | int) -> int:

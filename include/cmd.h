@@ -47,8 +47,10 @@ enum {
  *   CMD_DOPRI5_FIXED Dormand-Prince 5 tableau, fixed step, no error control
  *                    (the reference GPU "dopri5", integrator.cuh:186-228)
  *   CMD_RK45         controlled Dormand-Prince 5(4) with the CPU path's
- *                    Boost.Odeint step control (lattice.h:4072-4078)      */
-enum { CMD_RK4 = 0, CMD_DOPRI5_FIXED = 1, CMD_RK45 = 2 };
+ *                    Boost.Odeint step control (lattice.h:4072-4078)
+ *   CMD_CASH_KARP_FIXED  Cash-Karp 5 tableau, fixed step (the reference GPU
+ *                    "rk5" / "rkck54", integrator.cuh:141-185)            */
+enum { CMD_RK4 = 0, CMD_DOPRI5_FIXED = 1, CMD_RK45 = 2, CMD_CASH_KARP_FIXED = 3 };
 
 typedef struct cmd_handle cmd_handle;
 

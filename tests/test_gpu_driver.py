@@ -153,3 +153,33 @@ output_dir = {out}
         assert np.abs(sp[c] - ref).max() <= 1e-12 * max(1.0, ref.max())
     meta = json.loads((d / "metadata.json").read_text())
     assert meta["tau_steps"] == 5 and meta["pulse_amp"] == 0.4
+
+
+def test_driver_md_with_the_reference_example_integrator(driver, tmp_path):
+    """md_integrator = rk5 (the reference's example configs) runs the fixed-step Cash-Karp method."""
+    from classical_mcmc_spin_b200 import gpu_api
+    from classical_mcmc_spin_b200.lattice import Lattice
+    s0, init = _state_file(tmp_path, 72, 6)
+    out = tmp_path / "rk5"
+    _run(driver, tmp_path, f"""system = honeycomb_kitaev
+simulation_mode = molecular_dynamics
+lattice_size = 6,6,1
+field_strength = 0.7
+field_direction = 0.577,0.577,0.577
+md_time_start = 0.0
+md_time_end = 5.0
+md_timestep = 0.25
+md_save_interval = 1
+md_integrator = rk5
+initial_spin_config = {init}
+output_dir = {out}
+""")
+    d = out / "sample_0"
+    lat = Lattice.kitaev(6, 6, 1, h=0.7, field_direction=(0.577, 0.577, 0.577))
+    h = lat.to_gpu()
+    gpu_api.set_gpu_spins(h, s0)
+    traj, obs, times = gpu_api.integrate_gpu(h, 0.0, 5.0, 0.25, 1, "rk5")
+    np.testing.assert_array_equal(np.load(d / "trajectory_times.npy"), times)
+    np.testing.assert_array_equal(np.load(d / "trajectory_magnetization_local.npy"), obs[:, 3:6])
+    np.testing.assert_array_equal(np.load(d / "trajectory_spins.npy").reshape(len(times), -1),
+                                  np.stack([s for _, s in traj]))

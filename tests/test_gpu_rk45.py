@@ -94,6 +94,32 @@ def test_dopri5_fixed_matches_reference_gpu(api, oracle):
         assert np.abs(obs[r, :9] - o.magnetizations(rs[r])).max() <= 1e-13
 
 
+def test_cash_karp_fixed_matches_reference_gpu(api, oracle):
+    """The reference GPU "rk5" (Cash-Karp tableau, fixed step; the md_integrator of its example configs)."""
+    if not oracle.ref_available("libref_gpu.so"):
+        pytest.skip("oracle/_ref/libref_gpu.so not built")
+    lat, o = _kitaev(oracle, 6, 6)
+    s0 = _spins(lat.lattice_size, 35)
+    ref = oracle.RefGPU(o.ell(), o.n_atoms)
+    ref.set_spins(s0)
+    rt, rs = ref.integrate(0.0, 1.0, 0.01, save_interval=10, method="rk5")
+    ref.close()
+    h = lat.to_gpu()
+    api.set_gpu_spins(h, s0)
+    traj, obs, times = api.integrate_gpu(h, 0.0, 1.0, 0.01, 10, "rk5")
+    np.testing.assert_array_equal(times, rt)
+    assert np.abs(np.stack([s for _, s in traj]) - rs).max() <= 1e-12
+    for r in range(len(rt)):
+        assert np.abs(obs[r, :9] - o.magnetizations(rs[r])).max() <= 1e-13
+    api.set_gpu_spins(h, s0)                       # one step through cmd_step as well
+    api.step_gpu(h, 0.0, 0.01, "rk5")
+    ref = oracle.RefGPU(o.ell(), o.n_atoms)
+    ref.set_spins(s0)
+    ref.step(0.0, 0.01, method="rk5")
+    assert np.abs(api.get_gpu_spins(h) - ref.get_spins()).max() <= 1e-14
+    ref.close()
+
+
 def test_streamed_rk4_for_large_lattice(api, oracle):
     """48x48 honeycomb (4608 spins) does not fit one CTA: RK4 runs on a 4-CTA cluster."""
     lat, o = _kitaev(oracle, 48, 48)
