@@ -83,6 +83,7 @@ _SIGS = {
     "cmd_batch_rows": (C.c_int64, [C.c_int64, C.c_int64]),
     "cmd_run_batch_device": (C.c_int, [C.c_void_p, C.POINTER(BatchDesc), C.c_void_p, _I32]),
     "cmd_run_batch_device_noalloc": (C.c_int, [C.c_void_p, C.POINTER(BatchDesc), C.c_void_p, _I32]),
+    "cmd_max_dsdt_no_drive": (C.c_int, [C.c_void_p, _D]),
     "cmd_nonlinear_spectrum": (C.c_int, [_D, _D, _D, C.c_int64, C.c_int64, C.c_int32, _D, _D]),
     "cmd_layout_info": (C.c_int, [C.c_void_p, _I64]),
     "cmd_plan_layout": (C.c_int, [C.POINTER(LatticeDesc), _I64]),

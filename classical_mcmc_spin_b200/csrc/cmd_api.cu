@@ -1294,6 +1294,100 @@ int cmd_energy(cmd_handle* h, double* energy) {
     return CMD_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// max_c |(H_i x S_i)_c| over all sites with the drive off (Lattice::
+// max_dSdt_norm_no_drive, lattice_md.cpp:235-279): one thread per site (cell g,
+// atom at) of the AoS state; partners from the resident table's SoA offsets.
+// Non-negative doubles order like their bit patterns, so an integer atomicMax
+// gives the exact maximum in any order.
+template <int NAT, int Z, int LZ>
+__global__ void dsdt_max_kernel(const __grid_constant__ cmd::Couplings<NAT, Z> cp, const double* __restrict__ y,
+                                const int* __restrict__ nbr, int64_t G, unsigned long long* out) {
+    constexpr int NL = Z - LZ;
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double m = 0.0;
+    if (e < G * NAT) {
+        const int64_t g = e / NAT;
+        const int at = (int)(e - g * NAT);
+        auto spin = [&](int64_t gg, int aa, double (&P)[3]) {
+            const double* q = y + (gg * NAT + aa) * 3;
+            P[0] = q[0];
+            P[1] = q[1];
+            P[2] = q[2];
+        };
+        double S[3], H[3];
+        spin(g, at, S);
+        for (int d = 0; d < 3; ++d) H[d] = cp.has_field ? -cp.field[at][d] : 0.0;
+        if (cp.has_onsite)
+            for (int d = 0; d < 3; ++d)
+                cmd::bond_acc(H[d], 2.0 * cp.onsite[at][3 * d], 2.0 * cp.onsite[at][3 * d + 1],
+                              2.0 * cp.onsite[at][3 * d + 2], S[0], S[1], S[2]);
+        for (int n = 0; n < LZ; ++n) {
+            double P[3];
+            spin(g, (at + 1 + n) % NAT, P);
+            for (int d = 0; d < 3; ++d)
+                cmd::bond_acc(H[d], cp.J[at][n][3 * d], cp.J[at][n][3 * d + 1], cp.J[at][n][3 * d + 2], P[0], P[1],
+                              P[2]);
+        }
+        for (int mm = 0; mm < NL; ++mm) {
+            const int n = LZ + mm;
+            if (n >= cp.zc[at]) continue;
+            const int64_t off = nbr[(g * NAT + at) * NL + mm];
+            const int64_t ap = off / (3 * G), gp = off - ap * 3 * G;
+            double P[3];
+            spin(gp, (int)ap, P);
+            for (int d = 0; d < 3; ++d)
+                cmd::bond_acc(H[d], cp.J[at][n][3 * d], cp.J[at][n][3 * d + 1], cp.J[at][n][3 * d + 2], P[0], P[1],
+                              P[2]);
+        }
+        const double k0 = H[1] * S[2] - H[2] * S[1], k1 = H[2] * S[0] - H[0] * S[2], k2 = H[0] * S[1] - H[1] * S[0];
+        m = fmax(fabs(k0), fmax(fabs(k1), fabs(k2)));
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+template <int NAT, int Z, int LZ>
+int launch_dsdt_max(cmd_handle* h, unsigned long long* out) {
+    static const std::vector<double> zeros(3 * 64, 0.0);
+    cmd::Couplings<NAT, Z> cp;
+    fill_couplings<NAT, Z>(h, zeros.data(), zeros.data(), cp);
+    const int64_t n = h->lay.G * NAT;
+    dsdt_max_kernel<NAT, Z, LZ><<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(
+        cp, h->state.as<double>(), h->nbr.as<int>(), h->lay.G, out);
+    CUDA_TRY(cudaGetLastError());
+    return CMD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cmd_max_dsdt_no_drive(cmd_handle* h, double* out) {
+    cmd::clear_error();
+    if (int rc = check_handle(h, true)) return rc;
+    if (!out) return fail(CMD_ERR_INVALID_ARG, "NULL output");
+    if (h->NA > 64) return fail(CMD_ERR_UNSUPPORTED, "cells limited to 64 atoms");
+    if (int rc = h->scratch.ensure(sizeof(unsigned long long))) return rc;
+    auto* d = static_cast<unsigned long long*>(h->scratch.p);
+    CUDA_TRY(cudaMemsetAsync(d, 0, sizeof(unsigned long long), h->stream));
+    int rc = CMD_OK;
+    switch (global_type(h->lay)) {
+        case 0: rc = launch_dsdt_max<2, 3, 1>(h, d); break;
+        case 1: rc = launch_dsdt_max<4, 6, 3>(h, d); break;
+        default: return no_instance(h->lay);
+    }
+    if (rc != CMD_OK) return rc;
+    if (int rc2 = sync(h)) return rc2;
+    unsigned long long bits = 0;
+    CUDA_TRY(cudaMemcpy(&bits, d, sizeof(bits), cudaMemcpyDeviceToHost));
+    std::memcpy(out, &bits, sizeof(double));
+    return CMD_OK;
+}
+
 int cmd_normalize(cmd_handle* h, double spin_length) {
     cmd::clear_error();
     if (int rc = check_handle(h, true)) return rc;

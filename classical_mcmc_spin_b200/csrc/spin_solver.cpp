@@ -116,6 +116,8 @@ struct Config {
     std::vector<std::vector<double>> pump_directions = {{0.0, 1.0, 0.0}};
     std::vector<std::vector<double>> pump_directions_2;
     double tau_start = -200.0, tau_end = 200.0, tau_step = 1.0;
+    bool reuse_m0_for_m1 = true;                 // W1: M1(tau) as a time shift of M0 when stationary
+    double stationarity_tol = 1e-6;
     uint64_t seed = 0;
     bool cubic_cell = false;
     std::vector<std::string> ignored;
@@ -189,6 +191,8 @@ Config parse_file(const std::string& path) {
             else if (k == "tau_start") c.tau_start = std::stod(v);
             else if (k == "tau_end") c.tau_end = std::stod(v);
             else if (k == "tau_step") c.tau_step = std::stod(v);
+            else if (k == "reuse_m0_for_m1") c.reuse_m0_for_m1 = parse_bool(v);
+            else if (k == "stationarity_tol") c.stationarity_tol = std::stod(v);
             else if (k == "seed") c.seed = std::stoull(v);
             else if (k == "cubic_cell") c.cubic_cell = parse_bool(v);
             else {
@@ -488,17 +492,6 @@ void run_2dcs(const Config& c, Model& m) {
     const std::vector<double> d2 = c.pump_directions_2.empty() ? d1 : atom_dirs(c.pump_directions_2, m.na);
     std::vector<double> fd(2 * d1.size());
     check(cmd_lattice_rotate_pulse(m.L, d1.data(), d2.data(), fd.data()), "cmd_lattice_rotate_pulse");
-    // trajectories: 0 = M0 (pump at 0), 1 + 2k = M1(tau_k) (probe at tau_k), 2 + 2k = M01(tau_k)
-    const int64_t B = 1 + 2 * n_tau;
-    std::vector<double> t1((size_t)B, 0.0), t2((size_t)B, 0.0), a1((size_t)B, 0.0), a2((size_t)B, 0.0);
-    a1[0] = c.pump_amplitude;
-    for (int64_t k = 0; k < n_tau; ++k) {
-        t2[1 + 2 * k] = tau[k];
-        a2[1 + 2 * k] = c.pump_amplitude;
-        t2[2 + 2 * k] = tau[k];
-        a1[2 + 2 * k] = c.pump_amplitude;
-        a2[2 + 2 * k] = c.pump_amplitude;
-    }
     const fs::path dir = fs::path(c.output_dir) / "sample_0";
     fs::create_directories(dir);
     const std::vector<double> s0 = initial_state(c, m, 0);
@@ -506,6 +499,28 @@ void run_2dcs(const Config& c, Model& m) {
     check(cmd_set_spins(m.h, s0.data(), m.N * 3), "cmd_set_spins");
     double e_ground = 0.0;
     check(cmd_energy(m.h, &e_ground), "cmd_energy");
+    // W1 guard (lattice.h:5654-5676): a stationary ground state lets M1(tau)
+    // be M0 shifted in time; otherwise M1 is integrated (probe-only runs).
+    double max_ds = 0.0;
+    check(cmd_max_dsdt_no_drive(m.h, &max_ds), "cmd_max_dsdt_no_drive");
+    const bool synth = c.reuse_m0_for_m1 && max_ds <= c.stationarity_tol;
+    std::cout << "2dcs: max |dS/dt| without drive = " << max_ds << (synth ? " (stationary: M1 = shifted M0)\n"
+                                                                           : " (M1 integrated)\n");
+    const int64_t B = synth ? 1 + n_tau : 1 + 2 * n_tau;
+    // trajectories: 0 = M0 (pump at 0); synthesised: 1 + k = M01(tau_k); else
+    // 1 + 2k = M1(tau_k) (probe at tau_k), 2 + 2k = M01(tau_k)
+    std::vector<double> t1((size_t)B, 0.0), t2((size_t)B, 0.0), a1((size_t)B, 0.0), a2((size_t)B, 0.0);
+    a1[0] = c.pump_amplitude;
+    for (int64_t k = 0; k < n_tau; ++k) {
+        const int64_t i01 = synth ? 1 + k : 2 + 2 * k;
+        if (!synth) {
+            t2[1 + 2 * k] = tau[k];
+            a2[1 + 2 * k] = c.pump_amplitude;
+        }
+        t2[i01] = tau[k];
+        a1[i01] = c.pump_amplitude;
+        a2[i01] = c.pump_amplitude;
+    }
     std::vector<double> obs((size_t)B * n_t * 10);
     cmd_batch_desc bd;
     std::memset(&bd, 0, sizeof(bd));
@@ -527,6 +542,16 @@ void run_2dcs(const Config& c, Model& m) {
     bd.save_interval = 1;
     bd.obs = obs.data();
     check(cmd_run_batch(m.h, &bd), "cmd_run_batch");
+    // ground-state magnetisations (lattice.h:5649-5652): M_antiferro in the
+    // (-1)^i convention of magnetization_local_antiferro, M_local, M_global
+    double m_ground[9], row[10], ml[3], ms[3];
+    check(cmd_observables(m.h, row), "cmd_observables");
+    check(cmd_magnetization(m.h, ml, ms), "cmd_magnetization");
+    for (int d = 0; d < 3; ++d) {
+        m_ground[d] = ms[d];
+        m_ground[3 + d] = row[3 + d];
+        m_ground[6 + d] = row[6 + d];
+    }
     // datasets of pump_probe_spectroscopy.h5 (lattice.h:5749-5851)
     auto traj = [&](int64_t b, int off, double* out) {
         for (int64_t i = 0; i < n_t; ++i)
@@ -541,8 +566,23 @@ void run_2dcs(const Config& c, Model& m) {
         M1[q].assign((size_t)n_tau * n_t * 3, 0.0);
         M01[q].assign((size_t)n_tau * n_t * 3, 0.0);
         for (int64_t k = 0; k < n_tau; ++k) {
-            traj(1 + 2 * k, 3 * q, &M1[q][(size_t)k * n_t * 3]);
-            traj(2 + 2 * k, 3 * q, &M01[q][(size_t)k * n_t * 3]);
+            traj(synth ? 1 + k : 2 + 2 * k, 3 * q, &M01[q][(size_t)k * n_t * 3]);
+            if (!synth) {
+                traj(1 + 2 * k, 3 * q, &M1[q][(size_t)k * n_t * 3]);
+                continue;
+            }
+            // synthesize_M1_from_M0 (lattice_md.cpp:283-317): the ground state's
+            // magnetisation before tau, M0(t - tau) (nearest grid index) after
+            for (int64_t i = 0; i < n_t; ++i) {
+                double* dst = &M1[q][((size_t)k * n_t + i) * 3];
+                if (grid[i] < tau[k] + grid[0]) {
+                    for (int d = 0; d < 3; ++d) dst[d] = m_ground[3 * q + d];
+                } else {
+                    int64_t idx = (int64_t)std::llround((grid[i] - tau[k] - grid[0]) / c.md_timestep);
+                    idx = std::max<int64_t>(0, std::min<int64_t>(n_t - 1, idx));
+                    for (int d = 0; d < 3; ++d) dst[d] = M0[q][3 * idx + d];
+                }
+            }
         }
         write_npy(dir / (std::string("reference_M_") + names[q] + ".npy"), M0[q], {n_t, 3});
         write_npy(dir / (std::string("tau_scan_M1_") + names[q] + ".npy"), M1[q], {n_tau, n_t, 3});
@@ -564,6 +604,8 @@ void run_2dcs(const Config& c, Model& m) {
                .num("T_end", c.md_time_end).num("T_step", c.md_timestep).num("tau_start", c.tau_start)
                .num("tau_end", c.tau_end).num("tau_step", c.tau_step).num("tau_steps", (double)n_tau)
                .num("ground_state_energy", e_ground / (double)m.N).str("integration_method", "rk4")
+               .num("max_dsdt_no_drive", max_ds).num("stationarity_tol", c.stationarity_tol)
+               .num("m1_synthesized", synth ? 1 : 0)
                .done()
         << "\n";
     std::cout << "2dcs: " << n_tau << " delays x " << n_t << " times (" << B << " trajectories) -> " << dir.string()

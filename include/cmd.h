@@ -122,6 +122,11 @@ int cmd_normalize(cmd_handle* h, double spin_length);
  * (-1)^i staggered mean (lattice_gpu.cu:729-760), each [3]. */
 int cmd_magnetization(cmd_handle* h, double* mag_local, double* mag_staggered);
 
+/* Lattice::max_dSdt_norm_no_drive (lattice_md.cpp:235-279): the largest
+ * component |dS/dt| of the current state with the drive off -- the
+ * stationarity check that gates reusing M0 for M1(tau) in 2DCS. */
+int cmd_max_dsdt_no_drive(cmd_handle* h, double* out);
+
 /* Observables of the current state: one 10-double row (see top of file). */
 int cmd_observables(cmd_handle* h, double* row);
 

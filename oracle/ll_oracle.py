@@ -219,6 +219,9 @@ class OracleLattice:
         self._L.ora_local_field(self.h, _p(s), _p(out))
         return out
 
+    def max_dsdt_no_drive(self, state) -> float:
+        return float(self._L.ora_max_dsdt_no_drive(self.h, _p(_arr(state, 3 * self.N))))
+
     def energy(self, state) -> float:
         return float(self._L.ora_energy(self.h, _p(_arr(state, 3 * self.N))))
 

@@ -153,6 +153,7 @@ output_dir = {out}
         assert np.abs(sp[c] - ref).max() <= 1e-12 * max(1.0, ref.max())
     meta = json.loads((d / "metadata.json").read_text())
     assert meta["tau_steps"] == 5 and meta["pulse_amp"] == 0.4
+    assert meta["m1_synthesized"] == 0 and meta["max_dsdt_no_drive"] > 1e-3     # random state: M1 integrated
 
 
 def test_driver_md_with_the_reference_example_integrator(driver, tmp_path):
@@ -183,3 +184,60 @@ output_dir = {out}
     np.testing.assert_array_equal(np.load(d / "trajectory_magnetization_local.npy"), obs[:, 3:6])
     np.testing.assert_array_equal(np.load(d / "trajectory_spins.npy").reshape(len(times), -1),
                                   np.stack([s for _, s in traj]))
+
+
+def test_driver_2dcs_stationary_ground_state_reuses_m0(driver, tmp_path, oracle):
+    """A stationary state (all spins along the [111] field of the Kitaev-Gamma model) passes the W1 guard:
+    the batch holds M0 and M01 only and M1(tau) is M0 shifted in time (synthesize_M1_from_M0)."""
+    R = np.ones(3) / np.sqrt(3.0)
+    s0 = np.tile(R, 32)
+    init = tmp_path / "fm.txt"
+    np.savetxt(init, s0.reshape(-1, 3), fmt="%.17e")
+    out = tmp_path / "2dcs_fm"
+    _run(driver, tmp_path, f"""system = honeycomb_kitaev
+simulation_mode = 2dcs
+lattice_size = 4,4,1
+field_strength = 0.5
+field_direction = 1,1,1
+pump_direction = 0,0,1
+pump_amplitude = 0.4
+pump_width = 0.2
+pump_frequency = 0.5
+tau_start = 0.0
+tau_end = 0.6
+tau_step = 0.3
+md_time_start = -0.5
+md_time_end = 1.5
+md_timestep = 0.01
+initial_spin_config = {init}
+output_dir = {out}
+""")
+    d = out / "sample_0"
+    meta = json.loads((d / "metadata.json").read_text())
+    o = oracle.OracleLattice.kitaev(4, 4, 1, h=0.5, direction=R)
+    assert meta["m1_synthesized"] == 1
+    assert meta["max_dsdt_no_drive"] == pytest.approx(o.max_dsdt_no_drive(s0), abs=1e-15)
+    assert meta["max_dsdt_no_drive"] <= 1e-12
+    tau = np.load(d / "tau_scan_tau_values.npy")
+    times = np.load(d / "reference_times.npy")
+    n_t = len(times)
+    z = np.tile([0.0, 0.0, 1.0], 2)
+    B = 1 + len(tau)
+    t2 = np.concatenate([[0.0], tau])
+    s1 = np.ones(B)
+    s2 = np.concatenate([[0.0], np.ones(len(tau))])
+    _, obs = o.batch_rk4(np.tile(s0, (B, 1)), np.zeros(B), t2, s1, s2, 0.4, 0.2, 0.5, z, z, -0.5, 0.01, n_t - 1)
+    ground = {"antiferro": np.zeros(3), "local": R, "global": o.magnetizations(s0)[6:9]}
+    for q, name in enumerate(("antiferro", "local", "global")):
+        m0 = np.load(d / f"reference_M_{name}.npy")
+        m1 = np.load(d / f"tau_scan_M1_{name}.npy")
+        m01 = np.load(d / f"tau_scan_M01_{name}.npy")
+        assert np.abs(m0 - obs[0, :, 3 * q:3 * q + 3]).max() <= TOL_M
+        assert np.abs(m01 - obs[1:, :, 3 * q:3 * q + 3]).max() <= TOL_M
+        for k, tv in enumerate(tau):                 # lattice_md.cpp:283-317, restated
+            for i, t in enumerate(times):
+                if t < tv + times[0]:
+                    np.testing.assert_allclose(m1[k, i], ground[name], atol=1e-15)
+                else:
+                    idx = int(np.clip(np.round((t - tv - times[0]) / 0.01), 0, n_t - 1))
+                    np.testing.assert_array_equal(m1[k, i], m0[idx])

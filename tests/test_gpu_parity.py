@@ -294,3 +294,22 @@ def test_cubic_pyrochlore_cell_matches_oracle(api, oracle):
     assert np.abs(obs[:, :9] - rows[:, 1:10]).max() <= TOL_M
     assert np.abs(obs[:, 9] - rows[:, 10]).max() <= TOL_M
     assert np.abs(api.get_gpu_spins(h) - fin).max() <= TOL_S
+
+
+def test_max_dsdt_no_drive_matches_oracle(api, native, oracle):
+    """cmd_max_dsdt_no_drive (the 2DCS stationarity check) on random and stationary states, with a pulse set
+    (which it must ignore)."""
+    import ctypes as C
+    for kind, dims, kw in (("kitaev", (6, 6, 1), dict(h=0.3, field_direction=(0.0, 1.0, 0.0))),
+                           ("pyro", (2, 2, 2), dict(h=0.2, field_direction=R111, Jzz=1.0, Jpm=0.05, Jpmpm=0.02))):
+        lat, o = _pair(oracle, kind, dims, **kw)
+        h = lat.to_gpu()
+        fin = np.tile(R111, lat.N_atoms)
+        api.set_gpu_pulse(h, lat.rotate_pulse(fin, fin), 0.5, 0.5, 0.7, 0.0, 0.0)
+        for s0 in (_spins(lat.lattice_size, 40), np.tile(np.asarray(kw["field_direction"]) /
+                                                      np.linalg.norm(kw["field_direction"]), lat.lattice_size)):
+            api.set_gpu_spins(h, s0)
+            v = C.c_double()
+            native.check(native.lib().cmd_max_dsdt_no_drive(h.ptr, C.byref(v)), "max_dsdt")
+            ref = o.max_dsdt_no_drive(s0)
+            assert abs(v.value - ref) <= 1e-13 * max(1.0, ref), (kind, v.value, ref)
