@@ -26,6 +26,11 @@ CMD_RK4 = 0
 CMD_DOPRI5_FIXED = 1
 CMD_RK45 = 2
 CMD_CASH_KARP_FIXED = 3
+CMD_EULER = 4
+CMD_MIDPOINT = 5
+CMD_SSPRK53 = 6
+CMD_RK78 = 7
+CMD_BULIRSCH_STOER = 8
 
 STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "UNSUPPORTED", 3: "CUDA_ERROR", 4: "NONFINITE",
                 5: "WATCHDOG_TIMEOUT", 6: "OOM", 7: "STATE"}

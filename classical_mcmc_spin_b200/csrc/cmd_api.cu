@@ -827,7 +827,8 @@ int run_global(cmd_handle* owner, std::vector<GJob>& jobs, int mode, double abs_
         a.frames1 = src[1]->dframes.as<double>();
         a.afm1 = src[1]->dafm.as<double>();
     }
-    auto kern = cmd::rk_global_kernel<2, 3, 1, 4, 6, 3>;
+    auto kern = mode >= cmd::kModeEuler ? cmd::rk_global_kernel<2, 3, 1, 4, 6, 3, true>
+                                        : cmd::rk_global_kernel<2, 3, 1, 4, 6, 3, false>;
     int dev = 0, nsm = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -1105,11 +1106,21 @@ int run_single(cmd_handle* h, double T0, double dt, int64_t n_steps, int64_t sav
 namespace {
 
 int mode_of(int method) {
-    return method == CMD_RK45               ? cmd::kModeRK45
-           : method == CMD_DOPRI5_FIXED     ? cmd::kModeDopri5Fixed
-           : method == CMD_CASH_KARP_FIXED ? cmd::kModeCashKarpFixed
-                                            : cmd::kModeRK4;
+    switch (method) {
+        case CMD_RK45: return cmd::kModeRK45;
+        case CMD_DOPRI5_FIXED: return cmd::kModeDopri5Fixed;
+        case CMD_CASH_KARP_FIXED: return cmd::kModeCashKarpFixed;
+        case CMD_EULER: return cmd::kModeEuler;
+        case CMD_MIDPOINT: return cmd::kModeMidpoint;
+        case CMD_SSPRK53: return cmd::kModeSSPRK53;
+        case CMD_RK78: return cmd::kModeRK78;
+        case CMD_BULIRSCH_STOER: return cmd::kModeBulirschStoer;
+        default: return cmd::kModeRK4;
+    }
 }
+
+bool fixed_method(int method) { return method >= CMD_RK4 && method <= CMD_BULIRSCH_STOER && method != CMD_RK45; }
+bool known_method(int method) { return method >= CMD_RK4 && method <= CMD_BULIRSCH_STOER; }
 
 // One trajectory of the handle through the global-state integrator.
 int run_global_single(cmd_handle* h, int method, double T0, double T1, double dt, int64_t n_steps, int64_t save,
@@ -1145,9 +1156,8 @@ bool rk4_fits(const cmd_handle* h) { return resident_fits(h) || global_type(h->l
 int cmd_step(cmd_handle* h, double t, double dt, int method) {
     cmd::clear_error();
     if (int rc = check_handle(h, true)) return rc;
-    if (method != CMD_RK4 && method != CMD_DOPRI5_FIXED && method != CMD_CASH_KARP_FIXED)
-        return fail(CMD_ERR_INVALID_ARG,
-                    "cmd_step takes a fixed-step method (CMD_RK4, CMD_DOPRI5_FIXED or CMD_CASH_KARP_FIXED)");
+    if (!fixed_method(method))
+        return fail(CMD_ERR_INVALID_ARG, "cmd_step takes a fixed-step method (any but CMD_RK45)");
     if (!std::isfinite(t) || !std::isfinite(dt)) return fail(CMD_ERR_INVALID_ARG, "non-finite t or dt");
     if (method == CMD_RK4 && resident_fits(h)) return run_single(h, t, dt, 1, 1, (double)h->N, false, false, true);
     return run_global_single(h, method, t, t + dt, dt, 1, 1, 0, false, nullptr);
@@ -1157,8 +1167,7 @@ int cmd_integrate(cmd_handle* h, double T0, double T1, double dt, int64_t save_i
                   double* times, double* obs, double* states, int64_t max_rows, int64_t* rows_out) {
     cmd::clear_error();
     if (int rc = check_handle(h, true)) return rc;
-    if (method != CMD_RK4 && method != CMD_DOPRI5_FIXED && method != CMD_RK45 && method != CMD_CASH_KARP_FIXED)
-        return fail(CMD_ERR_INVALID_ARG, "unknown integration method");
+    if (!known_method(method)) return fail(CMD_ERR_INVALID_ARG, "unknown integration method");
     if (save_interval <= 0 || !(dt > 0.0) || !std::isfinite(T0) || !std::isfinite(T1))
         return fail(CMD_ERR_INVALID_ARG, "bad integration window");
     if (method == CMD_RK45) {
@@ -1213,8 +1222,7 @@ int cmd_run_uneven(cmd_traj_spec* specs, int64_t B, int method, double abs_tol, 
                    int64_t max_steps) {
     cmd::clear_error();
     if (!specs || B <= 0) return fail(CMD_ERR_INVALID_ARG, "empty batch");
-    if (method != CMD_RK4 && method != CMD_DOPRI5_FIXED && method != CMD_RK45 && method != CMD_CASH_KARP_FIXED)
-        return fail(CMD_ERR_INVALID_ARG, "unknown integration method");
+    if (!known_method(method)) return fail(CMD_ERR_INVALID_ARG, "unknown integration method");
     if (method == CMD_RK45 && (!(abs_tol >= 0.0) || !(rel_tol >= 0.0) || (abs_tol == 0.0 && rel_tol == 0.0)))
         return fail(CMD_ERR_INVALID_ARG, "bad tolerances");
     cmd_handle* owner = specs[0].lattice;

@@ -27,7 +27,10 @@
 
 namespace cmd {
 
-enum { kModeRK45 = 0, kModeDopri5Fixed = 1, kModeRK4 = 2, kModeCashKarpFixed = 3 };
+enum {
+    kModeRK45 = 0, kModeDopri5Fixed = 1, kModeRK4 = 2, kModeCashKarpFixed = 3,
+    kModeEuler = 4, kModeMidpoint = 5, kModeSSPRK53 = 6, kModeRK78 = 7, kModeBulirschStoer = 8
+};
 
 constexpr int kGVectors = 12;   // y, ynew, Ya, Yb, k1..k7, spare
 
@@ -137,7 +140,42 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* red, int used
     }
 }
 
-template <int NAT, int Z, int LZ>
+// Z = 1.0 * X + s[0] K[0], then Z = 1.0 * Z + s[j] K[j] for j = 1..M-1 over this thread's cells: the
+// rounding sequence of the reference's chain of update_arrays_kernel launches
+// (gpu_common_helpers.cu:10-20), each term added in the listed order.  Z may alias X.
+template <int M>
+__device__ __forceinline__ void lin_chain(double* Z, const double* X, const double* const (&K)[M],
+                                          const double (&s)[M], int G, int NE, int tid, int nt) {
+    for (int g = tid; g < G; g += nt)
+        for (int e = 0; e < NE; ++e) {
+            const long long i = (long long)e * G + g;
+            double v = 1.0 * X[i] + s[0] * K[0][i];
+#pragma unroll
+            for (int j = 1; j < M; ++j) v = 1.0 * v + s[j] * K[j][i];
+            Z[i] = v;
+        }
+}
+
+// Z = a1 X1 + a2 X2 (+ a3 X3) over this thread's cells (update_arrays[_three]_kernel,
+// gpu_common_helpers.cu:10-35).  Z may alias an input.
+__device__ __forceinline__ void lin2(double* Z, double a1, const double* X1, double a2, const double* X2, int G,
+                                     int NE, int tid, int nt) {
+    for (int g = tid; g < G; g += nt)
+        for (int e = 0; e < NE; ++e) {
+            const long long i = (long long)e * G + g;
+            Z[i] = a1 * X1[i] + a2 * X2[i];
+        }
+}
+__device__ __forceinline__ void lin3(double* Z, double a1, const double* X1, double a2, const double* X2, double a3,
+                                     const double* X3, int G, int NE, int tid, int nt) {
+    for (int g = tid; g < G; g += nt)
+        for (int e = 0; e < NE; ++e) {
+            const long long i = (long long)e * G + g;
+            Z[i] = a1 * X1[i] + a2 * X2[i] + a3 * X3[i];
+        }
+}
+
+template <int NAT, int Z, int LZ, bool XM>
 __device__ void run_trajectory(const Couplings<NAT, Z>& cp, const GTraj& T, const GArgs& a,
                                const double* frames, const double* afm, double* sh) {
     constexpr int NV = NVals<NAT>::value;
@@ -397,6 +435,153 @@ __device__ void run_trajectory(const Couplings<NAT, Z>& cp, const GTraj& T, cons
                         y[i] += (dt / 6.0) * (k[0][i] + 2.0 * k[1][i] + 2.0 * k[2][i] + k[3][i]);
                     }
                 __syncthreads();
+            } else if (XM && a.mode >= kModeEuler) {
+                // The reference GPU's other fixed-step methods, compiled only into the
+                // XM instance so the RK45 / RK4 / DOPRI5 kernel keeps its registers.
+                if constexpr (XM) {
+                    if (a.mode == kModeEuler) {  // integrator.cuh:91-99
+                    __syncthreads();
+                    lin2(y, 1.0, y, dt, k[0], G, NAT * 3, tid, nt);
+                    __syncthreads();
+                } else if (a.mode == kModeMidpoint) {   // "rk2" / "midpoint", integrator.cuh:100-114
+                    __syncthreads();
+                    lin2(Ya, 1.0, y, 0.5 * dt, k[0], G, NAT * 3, tid, nt);
+                    __syncthreads();
+                    rhs(Ya, k[1], t + 0.5 * dt, nullptr);
+                    lin2(y, 1.0, y, dt, k[1], G, NAT * 3, tid, nt);
+                    __syncthreads();
+                } else if (a.mode == kModeSSPRK53) {    // integrator.cuh:406-448; tmp = Ya, u = Yb
+                    // Five-stage third-order strong-stability-preserving tableau, the
+                    // reference's 15-digit coefficients.
+                    const double a30 = 0.355909775063327, a32 = 0.644090224936674;
+                    const double a40 = 0.367933791638137, a43 = 0.632066208361863;
+                    const double a52 = 0.237593836598569, a54 = 0.762406163401431;
+                    const double b10 = 0.377268915331368, b21 = 0.377268915331368, b32 = 0.242995220537396;
+                    const double b43 = 0.238458932846290, b54 = 0.287632146308408;
+                    const double c1 = 0.377268915331368, c2 = 0.754537830662736, c3 = 0.728985661612188;
+                    const double c4 = 0.699226135931670;
+                    __syncthreads();
+                    lin2(Ya, 1.0, y, b10 * dt, k[0], G, NAT * 3, tid, nt);
+                    __syncthreads();
+                    rhs(Ya, k[0], t + c1 * dt, nullptr);
+                    lin2(Yb, 1.0, Ya, b21 * dt, k[0], G, NAT * 3, tid, nt);
+                    __syncthreads();
+                    rhs(Yb, k[0], t + c2 * dt, nullptr);
+                    lin3(Ya, a30, y, a32, Yb, b32 * dt, k[0], G, NAT * 3, tid, nt);
+                    __syncthreads();
+                    rhs(Ya, k[0], t + c3 * dt, nullptr);
+                    lin3(yn, a40, y, a43, Ya, b43 * dt, k[0], G, NAT * 3, tid, nt);   // the reference updates tmp in place
+                    __syncthreads();
+                    rhs(yn, k[0], t + c4 * dt, nullptr);
+                    lin3(y, a52, Yb, a54, yn, b54 * dt, k[0], G, NAT * 3, tid, nt);
+                    __syncthreads();
+                } else if (a.mode == kModeRK78) {
+                    // The reference GPU "rk78" / "rkf78" (integrator.cuh:230-370): the first 11
+                    // stages of Fehlberg 7(8) and its 7th-order weights, every stage input a chain
+                    // of single-term updates.  Slots: k2 and k8 share k[1], k3 and k9 share k[2]
+                    // (k2 is dead after stage 3, k3 after stage 5), k10 = yn, k11 = Yb, tmp = Ya.
+                    double* const K1 = k[0];
+                    double* const K4 = k[3];
+                    double* const K5 = k[4];
+                    double* const K6 = k[5];
+                    double* const K7 = k[6];
+                    const int NE = NAT * 3;
+                    __syncthreads();
+                    { const double* const K[1] = {K1}; const double c[1] = {(2.0 / 27.0) * dt};
+                      lin_chain<1>(Ya, y, K, c, G, NE, tid, nt); }
+                    __syncthreads();
+                    rhs(Ya, k[1], t + (2.0 / 27.0) * dt, nullptr);                        // k2
+                    __syncthreads();
+                    { const double* const K[2] = {K1, k[1]}; const double c[2] = {(1.0 / 36.0) * dt, (1.0 / 12.0) * dt};
+                      lin_chain<2>(Ya, y, K, c, G, NE, tid, nt); }
+                    __syncthreads();
+                    rhs(Ya, k[2], t + (1.0 / 9.0) * dt, nullptr);                         // k3
+                    __syncthreads();
+                    { const double* const K[2] = {K1, k[2]}; const double c[2] = {(1.0 / 24.0) * dt, (1.0 / 8.0) * dt};
+                      lin_chain<2>(Ya, y, K, c, G, NE, tid, nt); }
+                    __syncthreads();
+                    rhs(Ya, K4, t + (1.0 / 6.0) * dt, nullptr);
+                    __syncthreads();
+                    { const double* const K[3] = {K1, K4, k[2]};
+                      const double c[3] = {(5.0 / 12.0) * dt, (-25.0 / 16.0) * dt, (25.0 / 16.0) * dt};
+                      lin_chain<3>(Ya, y, K, c, G, NE, tid, nt); }
+                    __syncthreads();
+                    rhs(Ya, K5, t + (5.0 / 12.0) * dt, nullptr);
+                    __syncthreads();
+                    { const double* const K[3] = {K1, K4, K5};
+                      const double c[3] = {(1.0 / 20.0) * dt, (1.0 / 4.0) * dt, (1.0 / 5.0) * dt};
+                      lin_chain<3>(Ya, y, K, c, G, NE, tid, nt); }
+                    __syncthreads();
+                    rhs(Ya, K6, t + (1.0 / 2.0) * dt, nullptr);
+                    __syncthreads();
+                    { const double* const K[4] = {K1, K4, K5, K6};
+                      const double c[4] = {(-25.0 / 108.0) * dt, (125.0 / 108.0) * dt, (-65.0 / 27.0) * dt,
+                                           (125.0 / 54.0) * dt};
+                      lin_chain<4>(Ya, y, K, c, G, NE, tid, nt); }
+                    __syncthreads();
+                    rhs(Ya, K7, t + (5.0 / 6.0) * dt, nullptr);
+                    __syncthreads();
+                    { const double* const K[4] = {K1, K5, K6, K7};
+                      const double c[4] = {(31.0 / 300.0) * dt, (61.0 / 225.0) * dt, (-2.0 / 9.0) * dt,
+                                           (13.0 / 900.0) * dt};
+                      lin_chain<4>(Ya, y, K, c, G, NE, tid, nt); }
+                    __syncthreads();
+                    rhs(Ya, k[1], t + (1.0 / 6.0) * dt, nullptr);                         // k8
+                    __syncthreads();
+                    { const double* const K[6] = {K1, K4, K5, K6, K7, k[1]};
+                      const double c[6] = {2.0 * dt, (-53.0 / 6.0) * dt, (704.0 / 45.0) * dt, (-107.0 / 9.0) * dt,
+                                           (67.0 / 90.0) * dt, 3.0 * dt};
+                      lin_chain<6>(Ya, y, K, c, G, NE, tid, nt); }
+                    __syncthreads();
+                    rhs(Ya, k[2], t + (2.0 / 3.0) * dt, nullptr);                         // k9
+                    __syncthreads();
+                    { const double* const K[7] = {K1, K4, K5, K6, K7, k[1], k[2]};
+                      const double c[7] = {(-91.0 / 108.0) * dt, (23.0 / 108.0) * dt, (-976.0 / 135.0) * dt,
+                                           (311.0 / 54.0) * dt, (-19.0 / 60.0) * dt, (17.0 / 6.0) * dt,
+                                           (-1.0 / 12.0) * dt};
+                      lin_chain<7>(Ya, y, K, c, G, NE, tid, nt); }
+                    __syncthreads();
+                    rhs(Ya, yn, t + (1.0 / 3.0) * dt, nullptr);                           // k10
+                    __syncthreads();
+                    { const double* const K[8] = {K1, K4, K5, K6, K7, k[1], k[2], yn};
+                      const double c[8] = {(2383.0 / 4100.0) * dt, (-341.0 / 164.0) * dt, (4496.0 / 1025.0) * dt,
+                                           (-301.0 / 82.0) * dt, (2133.0 / 4100.0) * dt, (45.0 / 82.0) * dt,
+                                           (45.0 / 164.0) * dt, (18.0 / 41.0) * dt};
+                      lin_chain<8>(Ya, y, K, c, G, NE, tid, nt); }
+                    __syncthreads();
+                    rhs(Ya, Yb, t + 1.0 * dt, nullptr);                                   // k11
+                    { const double* const K[7] = {K1, K6, K7, k[1], k[2], yn, Yb};
+                      const double c[7] = {(41.0 / 840.0) * dt, (34.0 / 105.0) * dt, (9.0 / 35.0) * dt,
+                                           (9.0 / 35.0) * dt, (9.0 / 280.0) * dt, (9.0 / 280.0) * dt,
+                                           (41.0 / 840.0) * dt};
+                      lin_chain<7>(y, y, K, c, G, NE, tid, nt); }
+                    __syncthreads();
+                } else if (a.mode == kModeBulirschStoer) {
+                    // The reference GPU "bulirsch_stoer" / "bs" (integrator.cuh:371-405): modified
+                    // midpoint over four substeps with the final smoothing step, no extrapolation.
+                    // y_prev / y_mid / y_next rotate over Ya, Yb and yn instead of being copied.
+                    const double hs = dt / 4;
+                    const int NE = NAT * 3;
+                    double* prev = y;
+                    double* mid = Ya;
+                    __syncthreads();
+                    lin2(mid, 1.0, y, hs, k[0], G, NE, tid, nt);
+                    __syncthreads();
+                    for (int sub = 1; sub < 4; ++sub) {
+                        rhs(mid, k[0], t + sub * hs, nullptr);
+                        double* next = (Ya != prev && Ya != mid) ? Ya : (Yb != prev && Yb != mid) ? Yb : yn;
+                        lin2(next, 1.0, prev, 2.0 * hs, k[0], G, NE, tid, nt);
+                        prev = mid;
+                        mid = next;
+                        __syncthreads();
+                    }
+                    rhs(mid, k[0], t + dt, nullptr);
+                    double* next = (Ya != prev && Ya != mid) ? Ya : (Yb != prev && Yb != mid) ? Yb : yn;
+                    lin2(next, 0.5, mid, 0.5, prev, G, NE, tid, nt);
+                    lin2(y, 1.0, next, 0.5 * hs, k[0], G, NE, tid, nt);
+                    __syncthreads();
+                    }
+                }
             } else {                            // integrator.cuh:141-228 arithmetic
                 __syncthreads();
                 for (int g = tid; g < G; g += nt)
@@ -463,7 +648,7 @@ __device__ void run_trajectory(const Couplings<NAT, Z>& cp, const GTraj& T, cons
     __syncthreads();
 }
 
-template <int NA0, int Z0, int LZ0, int NA1, int Z1, int LZ1>
+template <int NA0, int Z0, int LZ0, int NA1, int Z1, int LZ1, bool XM>
 __global__ void __launch_bounds__(256, 1)
 rk_global_kernel(const __grid_constant__ Couplings<NA0, Z0> c0, const __grid_constant__ Couplings<NA1, Z1> c1,
                  const __grid_constant__ GArgs a) {
@@ -476,8 +661,8 @@ rk_global_kernel(const __grid_constant__ Couplings<NA0, Z0> c0, const __grid_con
         __syncthreads();
         if (b >= a.B) break;
         const GTraj& T = a.traj[b];
-        if (T.type == 0) run_trajectory<NA0, Z0, LZ0>(c0, T, a, a.frames0, a.afm0, sh);
-        else run_trajectory<NA1, Z1, LZ1>(c1, T, a, a.frames1, a.afm1, sh);
+        if (T.type == 0) run_trajectory<NA0, Z0, LZ0, XM>(c0, T, a, a.frames0, a.afm0, sh);
+        else run_trajectory<NA1, Z1, LZ1, XM>(c1, T, a, a.frames1, a.afm1, sh);
     }
 }
 

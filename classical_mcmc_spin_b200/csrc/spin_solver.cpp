@@ -144,6 +144,25 @@ std::string normalise_mode(const std::string& v) {
     throw ConfigError("simulation_mode '" + s + "' is not on this path (molecular_dynamics, pump_probe, 2dcs)");
 }
 
+// md_integrator names of the reference GPU integrator (integrator.cuh:91-452); "dopri5" is
+// controlled (the CPU path's step control) under md_adaptive = true.  -1: not a method.
+const char* const kMethodNames =
+    "the GPU path (ssprk53, rk4, dopri5 / rk54 / rkf54, rk5 / rkck54, euler, rk2 / midpoint, rk78 / rkf78, "
+    "bs / bulirsch_stoer; md_adaptive = true makes dopri5 step-controlled)";
+
+int method_code(const std::string& m, bool adaptive) {
+    if (m == "rk4") return CMD_RK4;
+    if (m == "dopri5") return adaptive ? CMD_RK45 : CMD_DOPRI5_FIXED;
+    if (m == "rk54" || m == "rkf54") return CMD_DOPRI5_FIXED;
+    if (m == "rk5" || m == "rkck54") return CMD_CASH_KARP_FIXED;
+    if (m == "ssprk53") return CMD_SSPRK53;
+    if (m == "euler") return CMD_EULER;
+    if (m == "rk2" || m == "midpoint") return CMD_MIDPOINT;
+    if (m == "rk78" || m == "rkf78") return CMD_RK78;
+    if (m == "bs" || m == "bulirsch_stoer") return CMD_BULIRSCH_STOER;
+    return -1;
+}
+
 Config parse_file(const std::string& path) {
     std::ifstream f(path);
     if (!f) throw ConfigError("cannot open " + path);
@@ -219,10 +238,8 @@ Config parse_file(const std::string& path) {
     if (!(c.md_timestep > 0.0)) throw ConfigError("md_timestep must be positive");
     if (c.md_save_interval < 1) throw ConfigError("md_save_interval must be >= 1");
     if (c.num_trials < 1) throw ConfigError("num_trials must be >= 1");
-    if (c.mode != "2dcs" && c.md_integrator != "rk4" && c.md_integrator != "dopri5" && c.md_integrator != "rk5" &&
-        c.md_integrator != "rkck54")
-        throw ConfigError("md_integrator '" + c.md_integrator + "' is not on this path (rk4, rk5, dopri5; set "
-                          "md_adaptive = true for dopri5 with step control)");
+    if (c.mode != "2dcs" && method_code(c.md_integrator, c.md_adaptive) < 0)
+        throw ConfigError("md_integrator '" + c.md_integrator + "' is not a method of " + kMethodNames);
     for (int i = 0; i < 3; ++i)
         if (c.L[i] < 1) throw ConfigError("lattice_size entries must be >= 1");
     return c;
@@ -353,12 +370,9 @@ std::vector<double> atom_dirs(const std::vector<std::vector<double>>& dirs, int3
 }
 
 int method_of(const Config& c) {
-    const std::string& m = c.md_integrator;
-    if (m == "rk4") return CMD_RK4;
-    if (m == "dopri5") return c.md_adaptive ? CMD_RK45 : CMD_DOPRI5_FIXED;
-    if (m == "rk5" || m == "rkck54") return CMD_CASH_KARP_FIXED;
-    throw ConfigError("md_integrator '" + m + "' is not on this path (rk4, rk5, dopri5; set md_adaptive = true "
-                      "for dopri5 with step control)");
+    const int m = method_code(c.md_integrator, c.md_adaptive);
+    if (m < 0) throw ConfigError("md_integrator '" + c.md_integrator + "' is not a method of " + kMethodNames);
+    return m;
 }
 
 struct Rows {

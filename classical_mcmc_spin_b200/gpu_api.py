@@ -6,7 +6,8 @@ Same function names, argument meaning and result layout as
 Differences, by design: failures raise ``CmdError`` (the reference silently
 returns on a NULL handle or missing state, lattice_gpu.cu:660-723), the
 energy is implemented (the reference throws, lattice_gpu.cu:298-303), and an
-unknown method raises instead of falling back to ssprk53.
+unknown method raises instead of falling back to ssprk53.  The default method
+is the reference's, "ssprk53" (lattice_gpu_api.h:124, 139).
 """
 from __future__ import annotations
 
@@ -18,8 +19,14 @@ import numpy as np
 from . import _native as nat
 from ._native import check, dptr, f64, iptr
 
-METHODS = {"rk4": nat.CMD_RK4, "dopri5": nat.CMD_DOPRI5_FIXED, "rk45": nat.CMD_RK45,
-           "rk5": nat.CMD_CASH_KARP_FIXED, "rkck54": nat.CMD_CASH_KARP_FIXED}
+# The reference GPU method names (integrator.cuh:91-452) plus "rk45", the
+# controlled Dormand-Prince of the reference CPU path.
+METHODS = {"rk4": nat.CMD_RK4, "dopri5": nat.CMD_DOPRI5_FIXED, "rk54": nat.CMD_DOPRI5_FIXED,
+           "rkf54": nat.CMD_DOPRI5_FIXED, "rk45": nat.CMD_RK45,
+           "rk5": nat.CMD_CASH_KARP_FIXED, "rkck54": nat.CMD_CASH_KARP_FIXED,
+           "euler": nat.CMD_EULER, "rk2": nat.CMD_MIDPOINT, "midpoint": nat.CMD_MIDPOINT,
+           "ssprk53": nat.CMD_SSPRK53, "rk78": nat.CMD_RK78, "rkf78": nat.CMD_RK78,
+           "bulirsch_stoer": nat.CMD_BULIRSCH_STOER, "bs": nat.CMD_BULIRSCH_STOER}
 
 
 def _method(method: str | int) -> int:
@@ -138,7 +145,7 @@ def get_gpu_spins(handle) -> np.ndarray:
     return s
 
 
-def step_gpu(handle, t, dt, method="rk4"):
+def step_gpu(handle, t, dt, method="ssprk53"):
     check(nat.lib().cmd_step(handle.ptr, float(t), float(dt), _method(method)), "step_gpu")
 
 
@@ -147,15 +154,17 @@ def set_tolerances(handle, abs_tol, rel_tol, max_steps=0):
           "set_tolerances")
 
 
-def integrate_gpu(handle, T_start, T_end, dt, save_interval, method="rk4", with_states=True, max_rows=None):
+def integrate_gpu(handle, T_start, T_end, dt, save_interval, method="ssprk53", with_states=True, max_rows=None):
     """integrate_gpu (lattice_gpu_api.h:117-125).
 
     Returns ``(trajectory, obs, times)``: ``trajectory`` is the reference's list
     of ``(t, state)`` pairs (empty when ``with_states`` is False), ``obs`` the
     per-row observables {M_af, M_local, M_global, E/N} computed on the device.
-    Methods: "rk4", "dopri5" (the reference GPU's fixed-step Dormand-Prince)
-    and "rk45" (controlled Dormand-Prince with the CPU path's step control;
-    ``dt`` is the initial step, one row per accepted step).
+    Methods: the reference GPU's fixed-step ones ("ssprk53", the default,
+    "rk4", "dopri5" / "rk54", "rk5" / "rkck54", "euler", "rk2" / "midpoint",
+    "rk78" / "rkf78", "bs" / "bulirsch_stoer") and "rk45" (controlled
+    Dormand-Prince with the CPU path's step control; ``dt`` is the initial
+    step, one row per accepted step).
     """
     rows = C.c_int64()
     m = _method(method)

@@ -49,8 +49,22 @@ enum {
  *   CMD_RK45         controlled Dormand-Prince 5(4) with the CPU path's
  *                    Boost.Odeint step control (lattice.h:4072-4078)
  *   CMD_CASH_KARP_FIXED  Cash-Karp 5 tableau, fixed step (the reference GPU
- *                    "rk5" / "rkck54", integrator.cuh:141-185)            */
-enum { CMD_RK4 = 0, CMD_DOPRI5_FIXED = 1, CMD_RK45 = 2, CMD_CASH_KARP_FIXED = 3 };
+ *                    "rk5" / "rkck54", integrator.cuh:141-185)
+ * and the reference GPU's other fixed-step methods, same tableaux:
+ *   CMD_EULER        "euler" (integrator.cuh:91-99)
+ *   CMD_MIDPOINT     "rk2" / "midpoint" (integrator.cuh:100-114)
+ *   CMD_SSPRK53      "ssprk53", five-stage third-order SSP RK, the reference
+ *                    GPU API's default method (integrator.cuh:406-448)
+ *   CMD_RK78         "rk78" / "rkf78": the first 11 Fehlberg 7(8) stages with
+ *                    the 7th-order weights (integrator.cuh:230-370)
+ *   CMD_BULIRSCH_STOER  "bulirsch_stoer" / "bs": modified midpoint over four
+ *                    substeps plus smoothing, no extrapolation
+ *                    (integrator.cuh:371-405)
+ * ("rk54" / "rkf54" is CMD_DOPRI5_FIXED, integrator.cuh:450-452.)          */
+enum {
+    CMD_RK4 = 0, CMD_DOPRI5_FIXED = 1, CMD_RK45 = 2, CMD_CASH_KARP_FIXED = 3,
+    CMD_EULER = 4, CMD_MIDPOINT = 5, CMD_SSPRK53 = 6, CMD_RK78 = 7, CMD_BULIRSCH_STOER = 8
+};
 
 typedef struct cmd_handle cmd_handle;
 

@@ -85,7 +85,7 @@ seed = 12
     ("system = honeycomb_kitaev\nsimulation_mode = MD\npump_direction = 1,0\n", "multiple of 3"),
     ("system = honeycomb_kitaev\nsimulation_mode = MD\nmd_timestep = -1\n", "md_timestep"),
     ("system = honeycomb_kitaev\nsimulation_mode = MD\nthis line has no equals sign\n", "key = value"),
-    ("system = honeycomb_kitaev\nsimulation_mode = MD\nmd_integrator = rk78\n", "md_integrator"),
+    ("system = honeycomb_kitaev\nsimulation_mode = MD\nmd_integrator = rk99\n", "md_integrator"),
 ])
 def test_config_errors(driver, tmp_path, text, msg):
     r, _ = _parse(driver, tmp_path, text)

@@ -156,8 +156,10 @@ output_dir = {out}
     assert meta["m1_synthesized"] == 0 and meta["max_dsdt_no_drive"] > 1e-3     # random state: M1 integrated
 
 
-def test_driver_md_with_the_reference_example_integrator(driver, tmp_path):
-    """md_integrator = rk5 (the reference's example configs) runs the fixed-step Cash-Karp method."""
+@pytest.mark.parametrize("integrator", ["rk5", "ssprk53", "rk78", "bs"])
+def test_driver_md_with_the_reference_gpu_integrators(driver, tmp_path, integrator):
+    """md_integrator = rk5 (the reference's example configs: fixed-step Cash-Karp) and the reference
+    GPU's other fixed-step methods run as integrate_gpu with that method."""
     from classical_mcmc_spin_b200 import gpu_api
     from classical_mcmc_spin_b200.lattice import Lattice
     s0, init = _state_file(tmp_path, 72, 6)
@@ -171,7 +173,7 @@ md_time_start = 0.0
 md_time_end = 5.0
 md_timestep = 0.25
 md_save_interval = 1
-md_integrator = rk5
+md_integrator = {integrator}
 initial_spin_config = {init}
 output_dir = {out}
 """)
@@ -179,7 +181,7 @@ output_dir = {out}
     lat = Lattice.kitaev(6, 6, 1, h=0.7, field_direction=(0.577, 0.577, 0.577))
     h = lat.to_gpu()
     gpu_api.set_gpu_spins(h, s0)
-    traj, obs, times = gpu_api.integrate_gpu(h, 0.0, 5.0, 0.25, 1, "rk5")
+    traj, obs, times = gpu_api.integrate_gpu(h, 0.0, 5.0, 0.25, 1, integrator)
     np.testing.assert_array_equal(np.load(d / "trajectory_times.npy"), times)
     np.testing.assert_array_equal(np.load(d / "trajectory_magnetization_local.npy"), obs[:, 3:6])
     np.testing.assert_array_equal(np.load(d / "trajectory_spins.npy").reshape(len(times), -1),

@@ -230,7 +230,7 @@ def test_errors_are_status_codes(api, native):
     assert e.value.code == native.CMD_ERR_NONFINITE
     api.set_gpu_spins(h, _spins(lat.lattice_size, 1))
     with pytest.raises(ValueError):
-        api.step_gpu(h, 0.0, 0.01, "ssprk53")
+        api.step_gpu(h, 0.0, 0.01, "rk99")
     odd = Lattice.kitaev(4, 4, 1, J2_A=0.1, J2_B=0.1).to_gpu()    # 9 bonds/site: no kernel instance
     api.set_gpu_spins(odd, _spins(32, 1))
     with pytest.raises(CmdError) as e:
