@@ -27,7 +27,8 @@ class AdjointDesc(C.Structure):
     _fields_ = [("B", C.c_int64), ("states", C.c_void_p), ("T0", C.c_double), ("dt", C.c_double),
                 ("n_steps", C.c_int64), ("target", C.c_void_p), ("checkpoint_every", C.c_int64),
                 ("n_params", C.c_int32), ("forward_only", C.c_int32), ("dparams", C.c_void_p),
-                ("loss", C.c_void_p), ("grad", C.c_void_p), ("m_local", C.c_void_p)]
+                ("loss", C.c_void_p), ("grad", C.c_void_p), ("m_local", C.c_void_p), ("path", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 def _call(handle, desc):
@@ -53,8 +54,15 @@ def basis_lattices(build, n_params: int) -> list:
     return [build(np.eye(n_params)[q]) for q in range(n_params)]
 
 
-def adjoint_rk4(handle, dparams, states, T0, dt, n_steps, targets, checkpoint_every=0, forward_only=False):
-    """(loss[B], grad[B][n_params], m_local[B][n_steps+1][3]) through cmd_adjoint_rk4."""
+PATHS = {"auto": 0, "resident": 1, "streamed": 2, "global": 3}
+
+
+def adjoint_rk4(handle, dparams, states, T0, dt, n_steps, targets, checkpoint_every=0, forward_only=False,
+                path="auto"):
+    """(loss[B], grad[B][n_params], m_local[B][n_steps+1][3]) through cmd_adjoint_rk4.
+
+    ``path``: "auto" (resident when a CTA or cluster holds the lattice), or force "resident",
+    "streamed" or "global" (one CTA per trajectory, state in global memory)."""
     st = f64(states).reshape(-1, 3 * handle.N)
     B = st.shape[0]
     tg = f64(targets).reshape(B, n_steps + 1, 3)
@@ -79,6 +87,7 @@ def adjoint_rk4(handle, dparams, states, T0, dt, n_steps, targets, checkpoint_ev
     d.loss = loss.ctypes.data
     d.grad = grad.ctypes.data
     d.m_local = mloc.ctypes.data
+    d.path = PATHS[path]
     check(_call(handle, d), "cmd_adjoint_rk4")
     return loss, grad[:, :nq], mloc
 

@@ -15,6 +15,7 @@
 #include "rk4_cluster.cuh"
 #include "rk_global.cuh"
 #include "rk_adjoint.cuh"
+#include "rk_adjoint_cluster.cuh"
 #include "rk_stream.cuh"
 
 #include <cuda_runtime.h>
@@ -1610,6 +1611,21 @@ namespace {
 
 constexpr int kAdjParams = 5;
 
+// Derivative tables [q][atom][slot][9], [q][atom][3], [q][atom][9] into the kernel parameter block.
+template <int NAT, int Z, int NQ>
+void fill_param_derivs(const std::vector<double>& DJ, const std::vector<double>& DB, const std::vector<double>& DA,
+                       bool has_DA, cmd::ParamDerivs<NAT, Z, NQ>& pd) {
+    std::memset(&pd, 0, sizeof(pd));
+    for (int q = 0; q < NQ; ++q)
+        for (int at = 0; at < NAT; ++at) {
+            for (int s = 0; s < Z; ++s)
+                std::memcpy(pd.DJ[q][at][s], &DJ[(((size_t)q * NAT + at) * Z + s) * 9], 9 * sizeof(double));
+            std::memcpy(pd.DB[q][at], &DB[((size_t)q * NAT + at) * 3], 3 * sizeof(double));
+            std::memcpy(pd.DA[q][at], &DA[((size_t)q * NAT + at) * 9], 9 * sizeof(double));
+        }
+    pd.has_DA = has_DA;
+}
+
 template <int NAT, int Z, int LZ>
 int launch_adjoint(cmd_handle* h, const cmd::AdjArgs& a, const std::vector<double>& DJ, const std::vector<double>& DB,
                    const std::vector<double>& DA, bool has_DA, int64_t B) {
@@ -1619,18 +1635,88 @@ int launch_adjoint(cmd_handle* h, const cmd::AdjArgs& a, const std::vector<doubl
     CUDA_TRY(cudaGetLastError());
     if (a.forward_only) return CMD_OK;
     cmd::ParamDerivs<NAT, Z, kAdjParams> pd;
-    std::memset(&pd, 0, sizeof(pd));
-    for (int q = 0; q < kAdjParams; ++q)
-        for (int at = 0; at < NAT; ++at) {
-            for (int s = 0; s < Z; ++s)
-                std::memcpy(pd.DJ[q][at][s], &DJ[(((size_t)q * NAT + at) * Z + s) * 9], 9 * sizeof(double));
-            std::memcpy(pd.DB[q][at], &DB[((size_t)q * NAT + at) * 3], 3 * sizeof(double));
-            std::memcpy(pd.DA[q][at], &DA[((size_t)q * NAT + at) * 9], 9 * sizeof(double));
-        }
-    pd.has_DA = has_DA;
+    fill_param_derivs<NAT, Z, kAdjParams>(DJ, DB, DA, has_DA, pd);
     cmd::adjoint_backward_kernel<NAT, Z, LZ, kAdjParams><<<(unsigned)B, cmd::kAdjThreads, 0, h->stream>>>(cp, pd, a);
     CUDA_TRY(cudaGetLastError());
     return CMD_OK;
+}
+
+// Resident adjoint (rk_adjoint_cluster.cuh): one CTA or one cluster of CS CTAs per
+// trajectory, one thread per unit cell.
+using AdjClusterFn = int (*)(cmd_handle*, cmd::AdjClusterArgs, const std::vector<double>&, const std::vector<double>&,
+                             const std::vector<double>&, bool, int64_t);
+
+// Partner words of the cluster layout with CS CTAs (CS = 1: the global offsets, rank 0).
+const int* cluster_table(const cmd_handle* h, int cs) {
+    return cs == 1 ? h->nbr.as<int>() : static_cast<const int*>((cs == 2 ? h->cnbr2 : h->cnbr4).p);
+}
+
+template <int NAT, int Z, int LZ, int CS, int MAXT>
+int launch_adjoint_cluster(cmd_handle* h, cmd::AdjClusterArgs a, const std::vector<double>& DJ,
+                           const std::vector<double>& DB, const std::vector<double>& DA, bool has_DA, int64_t B) {
+    auto kern = cmd::adjoint_cluster_kernel<NAT, Z, LZ, CS, MAXT, kAdjParams>;
+    const int64_t G = h->lay.G, Gc = cluster_cells(G, CS);
+    const int threads = (int)((Gc + 31) / 32 * 32);
+    const size_t smem = (size_t)cmd::adj_cluster_smem_doubles(NAT, Gc) * sizeof(double);
+    if (threads > MAXT || smem > kMaxSmem) return fail(CMD_ERR_UNSUPPORTED, "lattice too large for this adjoint variant");
+    a.nbr = cluster_table(h, CS);
+    if (!a.nbr && !h->lay.nbr.empty()) return fail(CMD_ERR_UNSUPPORTED, "no cluster neighbour table for this lattice");
+    static bool attr_set = false;
+    if (!attr_set) {
+        CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
+        attr_set = true;
+    }
+    cmd::Couplings<NAT, Z> cp;
+    fill_couplings<NAT, Z>(h, h->fd.data(), h->fd.data() + 3 * h->NA, cp);
+    cmd::ParamDerivs<NAT, Z, kAdjParams> pd;
+    fill_param_derivs<NAT, Z, kAdjParams>(DJ, DB, DA, has_DA, pd);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(B * CS));
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = h->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CS;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, cp, pd, a, (int)Gc));
+    return CMD_OK;
+}
+
+struct AdjClusterVariant {
+    int NAT, Z, LZ, CS, MAXT;
+    AdjClusterFn fn;
+};
+
+const AdjClusterVariant kAdjClusterVariants[] = {
+    {2, 3, 1, 1, 576, &launch_adjoint_cluster<2, 3, 1, 1, 576>},
+    {2, 3, 1, 2, 576, &launch_adjoint_cluster<2, 3, 1, 2, 576>},
+    {2, 3, 1, 4, 576, &launch_adjoint_cluster<2, 3, 1, 4, 576>},
+    {4, 6, 3, 1, 256, &launch_adjoint_cluster<4, 6, 3, 1, 256>},
+    {4, 6, 3, 2, 256, &launch_adjoint_cluster<4, 6, 3, 2, 256>},
+    {4, 6, 3, 4, 256, &launch_adjoint_cluster<4, 6, 3, 4, 256>},
+};
+
+// The resident adjoint variant for h's lattice: the smallest cluster whose CTAs hold
+// the cells; -1 if none does.
+int pick_adjoint_cluster(const cmd_handle* h) {
+    const Layout& L = h->lay;
+    const int ty = global_type(L);
+    if (ty < 0) return -1;
+    for (int i = 0; i < (int)(sizeof(kAdjClusterVariants) / sizeof(kAdjClusterVariants[0])); ++i) {
+        const AdjClusterVariant& v = kAdjClusterVariants[i];
+        if ((ty == 0) != (v.NAT == 2)) continue;
+        const int64_t Gc = cluster_cells(L.G, v.CS);
+        if ((Gc + 31) / 32 * 32 > v.MAXT) continue;
+        if ((size_t)cmd::adj_cluster_smem_doubles(v.NAT, Gc) * sizeof(double) > kMaxSmem) continue;
+        if ((int64_t)v.NAT * 3 * Gc >= (1 << cmd::kClusterRankShift)) continue;
+        if (v.CS > 1 && !cluster_table(h, v.CS)) continue;
+        return i;
+    }
+    return -1;
 }
 
 
@@ -1806,6 +1892,7 @@ int cmd_adjoint_rk4(cmd_handle* h, const cmd_adjoint_desc* d) {
         return fail(CMD_ERR_INVALID_ARG, "bad adjoint description");
     if (d->n_params < 0 || d->n_params > kAdjParams || (d->n_params > 0 && (!d->dparams || !d->grad)))
         return fail(CMD_ERR_INVALID_ARG, "n_params must be 0..5 with derivative lattices and a grad buffer");
+    if (d->path < CMD_ADJ_AUTO || d->path > CMD_ADJ_GLOBAL) return fail(CMD_ERR_INVALID_ARG, "unknown adjoint path");
     const int ty = global_type(h->lay);
     if (ty < 0) return no_instance(h->lay);
     const int NA = h->NA, Z = h->lay.Z;
@@ -1881,12 +1968,37 @@ int cmd_adjoint_rk4(cmd_handle* h, const cmd_adjoint_desc* d) {
     a.width = h->width;
     a.freq = h->freq;
     a.forward_only = fwd_only;
-    // one CTA per trajectory when the batch fills the GPU, else streamed stages
+    // resident (one CTA or cluster per trajectory) when a variant holds the lattice; else one
+    // CTA per trajectory in global memory when the batch fills the GPU, else streamed stages
     const int cpt = cmd::kStreamTile / std::max(1, h->NA);
     const int tiles = (int)((h->lay.G + cpt - 1) / cpt);
-    const bool streamed = B < 148 && tiles >= 2 && B <= 65535;
+    const int resident = (d->path == CMD_ADJ_AUTO || d->path == CMD_ADJ_RESIDENT) ? pick_adjoint_cluster(h) : -1;
+    if (d->path == CMD_ADJ_RESIDENT && resident < 0)
+        return fail(CMD_ERR_UNSUPPORTED, "no resident adjoint variant holds this lattice");
+    const bool streamed = resident < 0 && B <= 65535 &&
+                          (d->path == CMD_ADJ_STREAMED || (d->path == CMD_ADJ_AUTO && B < 148 && tiles >= 2));
     int rc = CMD_OK;
-    if (streamed) {
+    if (resident >= 0) {
+        cmd::AdjClusterArgs ca{};
+        ca.traj = a.traj;
+        ca.G = a.G;
+        ca.n_steps = S;
+        ca.ckpt_every = C;
+        ca.dt = d->dt;
+        ca.forward_only = fwd_only;
+        if (h->amp != 0.0) {
+            const cmd::Pulse pl{h->t1, h->t2, h->amp, h->amp};
+            if (int rc2 = h->pulses.ensure(sizeof(cmd::Pulse))) return rc2;
+            if (int rc2 = h->drive.ensure((size_t)S * 6 * sizeof(double))) return rc2;
+            CUDA_TRY(cudaMemcpyAsync(h->pulses.p, &pl, sizeof(pl), cudaMemcpyHostToDevice, h->stream));
+            const int blocks = (int)std::min<int64_t>((S * 6 + 255) / 256, 148 * 32);
+            cmd::drive_table_kernel<<<blocks, 256, 0, h->stream>>>(h->pulses.as<cmd::Pulse>(), dtimes, S, d->dt,
+                                                                 h->width, h->freq, 1, h->drive.as<double>());
+            CUDA_TRY(cudaGetLastError());
+            ca.drive = h->drive.as<double>();
+        }
+        rc = kAdjClusterVariants[resident].fn(h, ca, DJ, DB, DA, has_DA, B);
+    } else if (streamed) {
         StreamAdjJob j{B, S, C, K, fwd_only, din, dtgt, dtimes, h->amloc.as<double>(), dout, d->dt};
         // the VJP carries as many parameter cotangents as requested (4 or 5)
         if (d->n_params <= 4)

@@ -284,7 +284,13 @@ int cmd_run_uneven(cmd_traj_spec* specs, int64_t B, int method, double abs_tol, 
  * dA/dtheta_q.  Checkpoints every checkpoint_every steps (0: ~sqrt(n_steps));
  * the backward sweep recomputes each segment.  forward_only != 0 runs only the
  * forward pass (loss, m_local; grad untouched).  Host pointers.
+ * path: CMD_ADJ_AUTO picks the resident kernel (one CTA or one thread-block
+ * cluster per trajectory, state on chip) when one holds the lattice, else one
+ * CTA per trajectory with the state in global memory when the batch fills the
+ * GPU, else streamed stages; the others force a path (CMD_ERR_UNSUPPORTED when
+ * CMD_ADJ_RESIDENT does not fit).
  */
+enum { CMD_ADJ_AUTO = 0, CMD_ADJ_RESIDENT = 1, CMD_ADJ_STREAMED = 2, CMD_ADJ_GLOBAL = 3 };
 typedef struct cmd_adjoint_desc {
     int64_t B;
     const double* states;              /* [B][N*3]                               */
@@ -298,6 +304,8 @@ typedef struct cmd_adjoint_desc {
     double* loss;                      /* [B] out                                */
     double* grad;                      /* [B][n_params] out                      */
     double* m_local;                   /* [B][n_steps+1][3] out, or NULL          */
+    int32_t path;                      /* CMD_ADJ_*                               */
+    int32_t reserved;
 } cmd_adjoint_desc;
 int cmd_adjoint_rk4(cmd_handle* h, const cmd_adjoint_desc* d);
 

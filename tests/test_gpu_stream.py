@@ -93,8 +93,10 @@ def test_pyrochlore_integrate_with_states(api, oracle, L, streamed):
     assert np.abs(api.get_gpu_spins(h) - fin).max() <= TOL_S
 
 
-def test_streamed_adjoint_kitaev_matches_tlm(native, oracle):
-    """24x24 honeycomb (576 cells: 5 tiles of 128), two trajectories: streamed forward, recompute and VJP."""
+@pytest.mark.parametrize("path", ["streamed", "auto"])
+def test_streamed_adjoint_kitaev_matches_tlm(native, oracle, path):
+    """24x24 honeycomb (576 cells: 5 tiles of 128), two trajectories: streamed forward, recompute and VJP,
+    and the resident kernel ("auto": one 576-thread CTA per trajectory)."""
     from classical_mcmc_spin_b200 import adjoint as adj
     theta = np.array([-1.0, 0.25, -0.02, 0.05, 0.1])
     build = lambda th: adj.kitaev_lattice(th, 24, 24)
@@ -104,7 +106,7 @@ def test_streamed_adjoint_kitaev_matches_tlm(native, oracle):
     states = np.stack([_spins(lat.lattice_size, 90 + b) for b in range(B)])
     targets = np.random.default_rng(9).normal(scale=0.05, size=(B, S + 1, 3))
     loss, grad, mloc = adj.adjoint_rk4(h, adj.basis_lattices(build, 5), states, 0.0, dt, S, targets,
-                                       checkpoint_every=7)
+                                       checkpoint_every=7, path=path)
     ob = lambda th: oracle.OracleLattice.kitaev(24, 24, 1, h=th[4], direction=(0, 1, 0), K=th[0], Gamma=th[1],
                                                 Gammap=th[2], J=th[3])
     base, basis = ob(theta), [ob(e) for e in np.eye(5)]
@@ -112,14 +114,16 @@ def test_streamed_adjoint_kitaev_matches_tlm(native, oracle):
         lt, gt = oracle.loss_grad_tlm(base, basis, states[b], 0.0, dt, S, targets[b])
         assert abs(loss[b] - lt) <= 1e-12 * max(1.0, abs(lt))
         np.testing.assert_allclose(grad[b], gt, rtol=1e-9, atol=1e-12)
-    # forward-only loss is the same streamed forward
-    lf, _, mf = adj.adjoint_rk4(h, [], states, 0.0, dt, S, targets, forward_only=True)
+    # forward-only loss is the same forward
+    lf, _, mf = adj.adjoint_rk4(h, [], states, 0.0, dt, S, targets, forward_only=True, path=path)
     np.testing.assert_array_equal(lf, loss)
     np.testing.assert_array_equal(mf, mloc)
 
 
-def test_streamed_adjoint_pyrochlore_matches_tlm(native, oracle):
-    """Pyrochlore 5^3 conventional cells (2000 spins, 500 cells: 8 tiles of 64) with a [111] field."""
+@pytest.mark.parametrize("path", ["streamed", "auto"])
+def test_streamed_adjoint_pyrochlore_matches_tlm(native, oracle, path):
+    """Pyrochlore 5^3 conventional cells (2000 spins, 500 cells: 8 tiles of 64) with a [111] field;
+    "auto" runs the resident kernel on a 2-CTA cluster."""
     from classical_mcmc_spin_b200 import adjoint as adj
     theta = np.array([1.0, 0.05, 0.02, 0.2])
     build = lambda th: adj.pyrochlore_lattice(th, 5, 5, 5, cubic=True)
@@ -129,7 +133,7 @@ def test_streamed_adjoint_pyrochlore_matches_tlm(native, oracle):
     states = _spins(lat.lattice_size, 91)[None, :]
     targets = np.random.default_rng(10).normal(scale=0.05, size=(1, S + 1, 3))
     loss, grad, _ = adj.adjoint_rk4(h, adj.basis_lattices(build, 4), states, 0.0, dt, S, targets,
-                                    checkpoint_every=4)
+                                    checkpoint_every=4, path=path)
     ob = lambda th: oracle.OracleLattice.pyrochlore_nk(5, 5, 5, h=th[3], direction=R111, cubic=True, Jzz=th[0],
                                                        Jpm=th[1], Jpmpm=th[2])
     lt, gt = oracle.loss_grad_tlm(ob(theta), [ob(e) for e in np.eye(4)], states[0], 0.0, dt, S, targets[0])
