@@ -228,15 +228,16 @@ def _adjoint_leg(torch, dev, build, theta, theta_target, n_params, B, S, dt, see
             "timing": "wall clock around the public call (host buffers in and out)"}
 
 
-def leg_adjoint_kitaev(torch, dev, S=20000):
-    """Adjoint: honeycomb 48x48 (4608 spins), 64 states (seed 4), RK4 dt 0.01, M_local loss against targets at
+def leg_adjoint_kitaev(torch, dev, S=20000, B=64):
+    """Adjoint: honeycomb 48x48 (4608 spins), B states (64 in the configuration; seed 4), RK4 dt 0.01, M_local
+    loss against targets at
     (K, G, G', J, h) = (-1, 0.3, -0.03, 0, 0.1); gradient at (-1, 0.25, -0.02, 0, 0) w.r.t. all five,
     checkpoint every 141 steps."""
     from classical_mcmc_spin_b200 import adjoint as A
     build = lambda th: A.kitaev_lattice(th, 48, 48)
     out = _adjoint_leg(torch, dev, build, np.array([-1.0, 0.25, -0.02, 0.0, 0.0]),
-                       np.array([-1.0, 0.3, -0.03, 0.0, 0.1]), 5, 64, S, 0.01, 4, 141)
-    out["workload"] = "adjoint_kitaev48x48_64traj_rk4"
+                       np.array([-1.0, 0.3, -0.03, 0.0, 0.1]), 5, B, S, 0.01, 4, 141)
+    out["workload"] = f"adjoint_kitaev48x48_{B}traj_rk4"
     return out
 
 
@@ -397,6 +398,7 @@ def main():
     ap.add_argument("--legs", default="uneven,adjoint,kitaev48,pyrochlore",
                     help="further workloads to time on rank 0 (comma list; empty for none)")
     ap.add_argument("--adjoint-steps", type=int, default=20000, help="RK4 steps of the 48x48 adjoint leg")
+    ap.add_argument("--adjoint-traj", type=int, default=64, help="trajectories of the 48x48 adjoint leg (config: 64)")
     ap.add_argument("--pyro-steps", type=int, default=20000, help="RK4 steps of the 65536-spin forward leg")
     ap.add_argument("--pyro-adjoint-steps", type=int, default=2000, help="RK4 steps of the 65536-spin adjoint")
     args = ap.parse_args()
@@ -576,7 +578,7 @@ def main():
         if "uneven" in want:
             legs["uneven_rk45"] = leg_uneven(torch, dev)
         if "adjoint" in want:
-            legs["adjoint_kitaev48"] = leg_adjoint_kitaev(torch, dev, S=args.adjoint_steps)
+            legs["adjoint_kitaev48"] = leg_adjoint_kitaev(torch, dev, S=args.adjoint_steps, B=args.adjoint_traj)
         if "kitaev48" in want:
             legs["kitaev48_forward"] = leg_kitaev48_forward(torch, dev)
         if "pyrochlore" in want:
