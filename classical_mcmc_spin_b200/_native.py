@@ -62,6 +62,20 @@ class TrajSpec(C.Structure):
                 ("stats", C.c_int64 * 4)]
 
 
+class MixedDesc(C.Structure):
+    """cmd_mixed_desc (include/cmd_mixed.h)."""
+    _fields_ = [("n_su2", C.c_int64), ("n_su3", C.c_int64), ("spin_dim_su2", C.c_int32),
+                ("spin_dim_su3", C.c_int32), ("n_atoms_su2", C.c_int32), ("n_atoms_su3", C.c_int32),
+                ("max_bilinear_su2", C.c_int32), ("max_bilinear_su3", C.c_int32), ("max_mixed_su2", C.c_int32),
+                ("max_mixed_su3", C.c_int32),
+                ("field_su2", C.c_void_p), ("onsite_su2", C.c_void_p), ("bilinear_su2", C.c_void_p),
+                ("partners_su2", C.c_void_p), ("counts_su2", C.c_void_p),
+                ("field_su3", C.c_void_p), ("onsite_su3", C.c_void_p), ("bilinear_su3", C.c_void_p),
+                ("partners_su3", C.c_void_p), ("counts_su3", C.c_void_p),
+                ("mixed_su2", C.c_void_p), ("mixed_partners_su3", C.c_void_p), ("mixed_counts_su2", C.c_void_p),
+                ("mixed_su3", C.c_void_p), ("mixed_partners_su2", C.c_void_p), ("mixed_counts_su3", C.c_void_p)]
+
+
 class CmdError(RuntimeError):
     def __init__(self, code: int, where: str, msg: str):
         super().__init__(f"{where}: {STATUS_NAMES.get(code, code)}: {msg}")
@@ -114,6 +128,18 @@ _SIGS = {
     "cmd_lattice_desc_of": (C.c_int, [C.c_void_p, C.POINTER(LatticeDesc)]),
     "cmd_lattice_rotate_pulse": (C.c_int, [C.c_void_p, _D, _D, _D]),
     "cmd_lattice_random_spins": (C.c_int, [C.c_int64, C.c_uint64, C.c_double, _D]),
+    "cmd_mixed_create": (C.c_int, [C.POINTER(MixedDesc), C.POINTER(C.c_void_p)]),
+    "cmd_mixed_destroy": (C.c_int, [C.c_void_p]),
+    "cmd_mixed_set_pulse": (C.c_int, [C.c_void_p, C.c_int32, _D, C.c_double, C.c_double, C.c_double, C.c_double,
+                                      C.c_double]),
+    "cmd_mixed_set_spins": (C.c_int, [C.c_void_p, _D, C.c_int64]),
+    "cmd_mixed_get_spins": (C.c_int, [C.c_void_p, _D, C.c_int64]),
+    "cmd_mixed_step": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_int]),
+    "cmd_mixed_integrate": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_int64, C.c_int, _D, _D,
+                                      C.c_int64, _I64]),
+    "cmd_mixed_magnetization": (C.c_int, [C.c_void_p, _D, _D, _D, _D]),
+    "cmd_mixed_normalize": (C.c_int, [C.c_void_p, C.c_double, C.c_double]),
+    "cmd_mixed_dims": (C.c_int, [C.c_void_p, _I64]),
     "cmd_lattice_free": (None, [C.c_void_p]),
 }
 

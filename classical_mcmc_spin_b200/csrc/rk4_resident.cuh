@@ -35,6 +35,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "drive.cuh"
+
 namespace cmd {
 
 template <int NAT, int Z>
@@ -116,11 +118,6 @@ __device__ __forceinline__ void drive_acc(double& h, double d1, double d2, doubl
     h = fma(-d2, f2, h);
 }
 
-// Drive envelope of lattice_md.cpp:45-56: a * exp(-(x/(2w))^2) * cos(freq x).
-__device__ __forceinline__ double drive_factor(double amp, double x, double width, double freq) {
-    const double u = x / (2.0 * width);
-    return amp * exp(-(u * u)) * cos(freq * x);
-}
 
 // Envelope table [B][n_steps][6]: for each step n the factors (pulse 1, pulse 2)
 // at t_n, t_n + dt/2 and t_n + dt, t_n the accumulated time of the reference loop.
