@@ -301,6 +301,37 @@ def leg_kitaev48_forward(torch, dev, S=20000):
     return out
 
 
+def leg_mixed(torch, dev, S=20000):
+    """Mixed SU(2)/SU(3) lattice shaped like TmFeO3: 6x6x6 cells of 4 SU(2) + 4 SU(3) atoms (864 + 864 sites;
+    seeded synthetic couplings, fields and on-site terms), one trajectory through the reference API's
+    integrate_mixed_gpu (mixed_gpu_api), dt 0.005, S steps, a two-pulse drive on both kinds of site; RK4 and the
+    reference default SSPRK53.  Wall clock around the call (one persistent launch; two saved rows)."""
+    from classical_mcmc_spin_b200 import mixed_gpu_api as mg
+    arr = mg.synthetic_mixed_lattice((6, 6, 6), seed=30)
+    h = mg.create_from(arr)
+    rng = np.random.default_rng(31)
+    mg.set_gpu_pulse_SU2(h, rng.normal(size=2 * arr["na2"] * 3), 0.5, 0.5, 1.0, 1.0, 2.0)
+    mg.set_gpu_pulse_SU3(h, rng.normal(size=2 * arr["na3"] * 8), 0.5, 0.5, 1.0, 1.0, 2.0)
+    y0 = mg.random_mixed_state(arr, 32)
+    sites = arr["n2"] + arr["n3"]
+    out = {"workload": "mixed_tmfeo3_shape_6x6x6_1728sites", "sites_su2": arr["n2"], "sites_su3": arr["n3"],
+           "steps": S, "dt": 0.005, "unit": "site·steps/s"}
+    for method, stages in (("rk4", 4), ("ssprk53", 5)):
+        mg.set_gpu_mixed_spins(h, y0)
+        mg.integrate_mixed_gpu(h, 0.0, 0.05, 0.005, 10, method)          # warm
+        mg.set_gpu_mixed_spins(h, y0)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        traj, _ = mg.integrate_mixed_gpu(h, 0.0, S * 0.005, 0.005, S, method)
+        s = time.perf_counter() - t0
+        y = traj[-1][1]
+        out[method] = {"s": s, "value": sites * S / s, "us_per_stage": s / (S * stages) * 1e6,
+                       "su2_norm_dev_max": float(np.abs(np.linalg.norm(y[:3 * arr["n2"]].reshape(-1, 3), axis=1)
+                                                        - 1).max())}
+    h.close()
+    return out
+
+
 def leg_pyrochlore(torch, dev, S=20000, S_adj=2000):
     """Large pyrochlore: 16^3 conventional cells (65536 spins), Jzz=1, J+-=0.05, J+-+-=0.02, h=0.2 along [111],
     32 states (seed 5), RK4 dt 0.005.  Forward through cmd_run_batch_device (device buffers, CUDA events, M and E
@@ -395,10 +426,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
     ap.add_argument("--no-peak", action="store_true", help="skip the DGEMM peak probe (profiling runs)")
-    ap.add_argument("--legs", default="uneven,adjoint,kitaev48,pyrochlore",
+    ap.add_argument("--legs", default="uneven,adjoint,kitaev48,pyrochlore,mixed",
                     help="further workloads to time on rank 0 (comma list; empty for none)")
     ap.add_argument("--adjoint-steps", type=int, default=20000, help="RK4 steps of the 48x48 adjoint leg")
     ap.add_argument("--adjoint-traj", type=int, default=64, help="trajectories of the 48x48 adjoint leg (config: 64)")
+    ap.add_argument("--mixed-steps", type=int, default=20000, help="steps of the mixed SU(2)/SU(3) leg")
     ap.add_argument("--pyro-steps", type=int, default=20000, help="RK4 steps of the 65536-spin forward leg")
     ap.add_argument("--pyro-adjoint-steps", type=int, default=2000, help="RK4 steps of the 65536-spin adjoint")
     args = ap.parse_args()
@@ -581,6 +613,8 @@ def main():
             legs["adjoint_kitaev48"] = leg_adjoint_kitaev(torch, dev, S=args.adjoint_steps, B=args.adjoint_traj)
         if "kitaev48" in want:
             legs["kitaev48_forward"] = leg_kitaev48_forward(torch, dev)
+        if "mixed" in want:
+            legs["mixed_tmfeo3_shape"] = leg_mixed(torch, dev, S=args.mixed_steps)
         if "pyrochlore" in want:
             legs["pyrochlore65536"] = leg_pyrochlore(torch, dev, S=args.pyro_steps, S_adj=args.pyro_adjoint_steps)
 

@@ -14,9 +14,11 @@
 // reference.
 //
 // One trajectory per launch, persistent for the whole run: a thread-block cluster
-// of CS CTAs, one site per thread (more when the lattice is larger), the state and
-// the stage vectors in global memory (L2-resident at these sizes), the cluster
-// barrier between stages; the steps are rk_fixed.cuh's.  The reference launches
+// of CS CTAs (up to 16, a non-portable size the host checks before using), one
+// site per thread (more when the lattice is larger), the state and
+// the stage vectors in global memory (L2-resident at these sizes), the distinct
+// couplings in shared memory, the cluster barrier between stages; the steps are
+// rk_fixed.cuh's.  The reference launches
 // two RHS kernels and an update kernel per stage with a device synchronisation
 // after each.
 #pragma once
@@ -30,23 +32,32 @@ namespace cmd {
 
 namespace mcg = cooperative_groups;
 
+// Couplings are stored once per distinct value: `tab` holds the distinct fields,
+// on-site matrices, like-site and mixed bond matrices of each kind (offsets off_*),
+// and per-site / per-(slot, site) indices pick them (index arrays site-minor, so a
+// warp's loads coalesce).  The kernel copies `tab` into shared memory when it fits.
 struct MixedDev {
     int N2, N3, NA2, NA3;                  // sites and atoms per cell of each kind
     int z2, z3, zm2, zm3;                  // ELL widths: like-site bonds, mixed bonds
-    const double* field2;                  // [N2][3]
-    const double* onsite2;                 // [N2][9]
-    const double* bil2;                    // [N2][z2][9]
-    const int* part2;                      // [N2][z2] SU(2) partner or -1
+    const double* tab;                     // distinct couplings (global memory), block strides kStride*
+    int tab_doubles, tab_in_smem;
+    const int* order;                      // [N2 + N3] site of each work slot: the kinds alternate by warp
+    int off_f2, off_o2, off_b2, off_m2;    // offsets in tab: fields [3], on-site [9], bonds [9], mixed [3*8]
+    int off_f3, off_o3, off_b3, off_m3;    //                 fields [8], on-site [64], bonds [64], mixed [8*3]
+    const int* f2i;                        // [N2] field index
+    const int* o2i;                        // [N2] on-site index
+    const int* b2i;                        // [z2][N2] bond matrix index
+    const int* part2;                      // [z2][N2] SU(2) partner or -1
     const int* cnt2;                       // [N2]
-    const double* mix2;                    // [N2][zm2][3*8]
-    const int* mpart2;                     // [N2][zm2] SU(3) partner or -1
+    const int* m2i;                        // [zm2][N2] mixed matrix index
+    const int* mpart2;                     // [zm2][N2] SU(3) partner or -1
     const int* mcnt2;                      // [N2]
-    const double* field3;                  // [N3][8]
-    const double* onsite3;                 // [N3][64]
-    const double* bil3;                    // [N3][z3][64]
+    const int* f3i;
+    const int* o3i;
+    const int* b3i;                        // [z3][N3]
     const int* part3;
     const int* cnt3;
-    const double* mix3;                    // [N3][zm3][8*3]
+    const int* m3i;                        // [zm3][N3]
     const int* mpart3;                     // SU(2) partner or -1
     const int* mcnt3;
     const double* drive2;                  // [2][NA2][3]
@@ -54,6 +65,11 @@ struct MixedDev {
     double amp2, width2, freq2, t1_2, t2_2;
     double amp3, width3, freq3, t1_3, t2_3;
 };
+
+// Doubles between consecutive distinct blocks of each table: odd, so lanes reading
+// different blocks at the same offset fall in different shared-memory banks.
+constexpr int kStrideF2 = 3, kStrideO2 = 9, kStrideB2 = 9, kStrideM = 25;
+constexpr int kStrideF3 = 9, kStrideO3 = 65, kStrideB3 = 65;
 
 struct MixedRun {
     double* work;              // 11 vectors of V doubles: y, k[0..6], Ya, Yb, yn
@@ -85,35 +101,37 @@ __device__ __forceinline__ void su3_cross(double (&r)[8], const double (&a)[8], 
     }
 }
 
-// dS/dt of site s (SU(2) sites first, then SU(3)) at state Y; f = drive factors
-// (SU(2) pulse 1, pulse 2, SU(3) pulse 1, pulse 2) of the stage time.
-__device__ __forceinline__ void mixed_rhs_site(const MixedDev& m, const double* __restrict__ Y,
+// dS/dt of site s (SU(2) sites first, then SU(3)) at state Y; T = the distinct-coupling
+// table (shared or global memory); f = drive factors (SU(2) pulse 1, pulse 2, SU(3)
+// pulse 1, pulse 2) of the stage time.
+__device__ __forceinline__ void mixed_rhs_site(const MixedDev& m, const double* T, const double* __restrict__ Y,
                                                double* __restrict__ K, int s, const double (&f)[4]) {
     const double* Y3 = Y + 3LL * m.N2;
     if (s < m.N2) {
         double S[3], H[3];
+        const double* B = T + m.off_f2 + kStrideF2 * m.f2i[s];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             S[d] = Y[3LL * s + d];
-            H[d] = -m.field2[3LL * s + d];
+            H[d] = -B[d];
         }
-        const double* A = m.onsite2 + 9LL * s;
+        const double* A = T + m.off_o2 + kStrideO2 * m.o2i[s];
 #pragma unroll
         for (int i = 0; i < 3; ++i) H[i] += 2.0 * (A[3 * i] * S[0] + A[3 * i + 1] * S[1] + A[3 * i + 2] * S[2]);
         const int nb = min(m.cnt2[s], m.z2);
         for (int n = 0; n < nb; ++n) {
-            const int p = m.part2[(long long)s * m.z2 + n];
+            const int p = m.part2[(long long)n * m.N2 + s];
             if (p < 0) continue;
-            const double* J = m.bil2 + ((long long)s * m.z2 + n) * 9;
+            const double* J = T + m.off_b2 + kStrideB2 * m.b2i[(long long)n * m.N2 + s];
             const double P0 = Y[3LL * p], P1 = Y[3LL * p + 1], P2 = Y[3LL * p + 2];
 #pragma unroll
             for (int i = 0; i < 3; ++i) H[i] += J[3 * i] * P0 + J[3 * i + 1] * P1 + J[3 * i + 2] * P2;
         }
         const int nm = min(m.mcnt2[s], m.zm2);
         for (int n = 0; n < nm; ++n) {
-            const int p = m.mpart2[(long long)s * m.zm2 + n];
+            const int p = m.mpart2[(long long)n * m.N2 + s];
             if (p < 0) continue;
-            const double* M = m.mix2 + ((long long)s * m.zm2 + n) * 24;
+            const double* M = T + m.off_m2 + kStrideM * m.m2i[(long long)n * m.N2 + s];
             double P[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) P[j] = Y3[8LL * p + j];
@@ -137,12 +155,13 @@ __device__ __forceinline__ void mixed_rhs_site(const MixedDev& m, const double* 
     } else {
         const int s3 = s - m.N2;
         double S[8], H[8];
+        const double* B = T + m.off_f3 + kStrideF3 * m.f3i[s3];
 #pragma unroll
         for (int d = 0; d < 8; ++d) {
             S[d] = Y3[8LL * s3 + d];
-            H[d] = -m.field3[8LL * s3 + d];
+            H[d] = -B[d];
         }
-        const double* A = m.onsite3 + 64LL * s3;
+        const double* A = T + m.off_o3 + kStrideO3 * m.o3i[s3];
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             double t = 0.0;
@@ -152,9 +171,9 @@ __device__ __forceinline__ void mixed_rhs_site(const MixedDev& m, const double* 
         }
         const int nb = min(m.cnt3[s3], m.z3);
         for (int n = 0; n < nb; ++n) {
-            const int p = m.part3[(long long)s3 * m.z3 + n];
+            const int p = m.part3[(long long)n * m.N3 + s3];
             if (p < 0) continue;
-            const double* J = m.bil3 + ((long long)s3 * m.z3 + n) * 64;
+            const double* J = T + m.off_b3 + kStrideB3 * m.b3i[(long long)n * m.N3 + s3];
             double P[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) P[j] = Y3[8LL * p + j];
@@ -168,9 +187,9 @@ __device__ __forceinline__ void mixed_rhs_site(const MixedDev& m, const double* 
         }
         const int nm = min(m.mcnt3[s3], m.zm3);
         for (int n = 0; n < nm; ++n) {
-            const int p = m.mpart3[(long long)s3 * m.zm3 + n];
+            const int p = m.mpart3[(long long)n * m.N3 + s3];
             if (p < 0) continue;
-            const double* M = m.mix3 + ((long long)s3 * m.zm3 + n) * 24;
+            const double* M = T + m.off_m3 + kStrideM * m.m3i[(long long)n * m.N3 + s3];
             const double P0 = Y[3LL * p], P1 = Y[3LL * p + 1], P2 = Y[3LL * p + 2];
 #pragma unroll
             for (int i = 0; i < 8; ++i) H[i] += M[3 * i] * P0 + M[3 * i + 1] * P1 + M[3 * i + 2] * P2;
@@ -189,7 +208,7 @@ __device__ __forceinline__ void mixed_rhs_site(const MixedDev& m, const double* 
 }
 
 // Steps over one cluster: every thread of the cluster owns the elements of a strided
-// share of the sites, the barrier is the cluster's.
+// share of the work slots (sites through MixedDev::order), the barrier is the cluster's.
 template <class R, class E>
 struct ClusterStepCtx {
     const R& rhs_f;
@@ -207,6 +226,7 @@ __global__ void __launch_bounds__(kMixedThreads, 1)
 mixed_integrate_kernel(const __grid_constant__ MixedDev m, const __grid_constant__ MixedRun r) {
     mcg::cluster_group cluster = mcg::this_cluster();
     __shared__ double fs[4];
+    extern __shared__ double stab[];       // the distinct couplings, when they fit
     const int nt = (int)blockDim.x * CS;
     const int gt = (int)cluster.block_rank() * (int)blockDim.x + (int)threadIdx.x;
     const long long V = 3LL * m.N2 + 8LL * m.N3;
@@ -220,6 +240,7 @@ mixed_integrate_kernel(const __grid_constant__ MixedDev m, const __grid_constant
     double* Yb = r.work + 9 * V;
     double* yn = r.work + 10 * V;
 
+    const double* T = m.tab_in_smem ? stab : m.tab;
     // every rhs call is preceded by a cluster barrier, so fs is free to rewrite
     auto rhs = [&](const double* Yin, double* K, double ts) {
         if (driven) {
@@ -234,12 +255,13 @@ mixed_integrate_kernel(const __grid_constant__ MixedDev m, const __grid_constant
         }
         const double f[4] = {driven ? fs[0] : 0.0, driven ? fs[1] : 0.0, driven ? fs[2] : 0.0,
                              driven ? fs[3] : 0.0};
-        for (int s = gt; s < sites; s += nt) mixed_rhs_site(m, Yin, K, s, f);
+        for (int q = gt; q < sites; q += nt) mixed_rhs_site(m, T, Yin, K, m.order[q], f);
     };
     // the elements of the thread's own sites: the ones its rhs writes (rk_fixed.cuh reads
     // a stage derivative right after the rhs that wrote it, without a barrier)
     auto each = [&](auto&& f) {
-        for (int s = gt; s < sites; s += nt) {
+        for (int q = gt; q < sites; q += nt) {
+            const int s = m.order[q];
             if (s < m.N2) {
                 const long long b = 3LL * s;
                 f(b);
@@ -254,6 +276,8 @@ mixed_integrate_kernel(const __grid_constant__ MixedDev m, const __grid_constant
     };
     const ClusterStepCtx<decltype(rhs), decltype(each)> ctx{rhs, each};
 
+    if (m.tab_in_smem)
+        for (int i = threadIdx.x; i < m.tab_doubles; i += blockDim.x) stab[i] = m.tab[i];
     each([&](long long i) { y[i] = r.y0[i]; });
     cluster.sync();
     double t = r.T0;

@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -57,25 +58,58 @@ struct cmd_mixed {
 
 namespace {
 
-int upload(cmd_mixed* h, const void* src, size_t bytes, char*& cursor) {
-    if (bytes) MIX_TRY(cudaMemcpyAsync(cursor, src, bytes, cudaMemcpyHostToDevice, h->stream));
-    cursor += (bytes + 255) / 256 * 256;
-    return CMD_OK;
-}
-
 size_t pad(size_t bytes) { return (bytes + 255) / 256 * 256; }
 
-// Partner tables as int32, -1 where the partner lies outside [0, limit).
-std::vector<int> partners(const int64_t* p, size_t n, int64_t limit) {
-    std::vector<int> out(n, -1);
-    for (size_t i = 0; i < n; ++i)
-        if (p && p[i] >= 0 && p[i] < limit) out[i] = (int)p[i];
-    return out;
-}
-std::vector<int> counts(const int64_t* c, size_t n) {
-    std::vector<int> out(n, 0);
-    for (size_t i = 0; i < n; ++i) out[i] = c ? (int)std::max<int64_t>(0, std::min<int64_t>(c[i], 1 << 30)) : 0;
-    return out;
+constexpr size_t kMixedSmemMax = 200 * 1024;   // distinct couplings copied to shared memory up to this size
+
+// Distinct blocks of w doubles in first-seen order, and the index of each block added.
+struct Distinct {
+    int w;
+    std::vector<double> vals;
+    std::map<std::vector<double>, int> seen;
+    explicit Distinct(int w_) : w(w_) {}
+    int add(const double* p) {
+        std::vector<double> k(p, p + w);
+        auto it = seen.find(k);
+        if (it != seen.end()) return it->second;
+        const int id = (int)(vals.size() / w);
+        vals.insert(vals.end(), k.begin(), k.end());
+        seen.emplace(std::move(k), id);
+        return id;
+    }
+};
+
+// One kind of site: distinct field / on-site / bond / mixed-bond blocks, and the
+// per-site and per-(slot, site) indices (slot-major: index n * N + s).
+struct KindTables {
+    std::vector<int> fi, oi, bi, part, cnt, mi, mpart, mcnt;
+};
+
+void build_kind(int64_t N, int z, int zm, int dim, const double* field, const double* onsite,
+                const double* bil, const int64_t* partners, const int64_t* counts, int64_t limit_same,
+                const double* mix, const int64_t* mpartners, const int64_t* mcounts, int64_t limit_other,
+                Distinct& F, Distinct& O, Distinct& B, Distinct& M, KindTables& t) {
+    t.fi.assign(N, 0); t.oi.assign(N, 0); t.cnt.assign(N, 0); t.mcnt.assign(N, 0);
+    t.bi.assign((size_t)N * z, 0); t.part.assign((size_t)N * z, -1);
+    t.mi.assign((size_t)N * zm, 0); t.mpart.assign((size_t)N * zm, -1);
+    for (int64_t s = 0; s < N; ++s) {
+        t.fi[s] = F.add(field + (size_t)s * dim);
+        t.oi[s] = O.add(onsite + (size_t)s * dim * dim);
+        t.cnt[s] = (int)std::max<int64_t>(0, std::min<int64_t>(counts[s], z));
+        for (int n = 0; n < t.cnt[s]; ++n) {
+            const int64_t p = partners[(size_t)s * z + n];
+            if (p < 0 || p >= limit_same) continue;
+            t.part[(size_t)n * N + s] = (int)p;
+            t.bi[(size_t)n * N + s] = B.add(bil + ((size_t)s * z + n) * dim * dim);
+        }
+        t.mcnt[s] = zm > 0 ? (int)std::max<int64_t>(0, std::min<int64_t>(mcounts[s], zm)) : 0;
+        for (int n = 0; n < t.mcnt[s]; ++n) {
+            const int64_t p = mpartners[(size_t)s * zm + n];
+            if (p < 0 || p >= limit_other) continue;
+            t.mpart[(size_t)n * N + s] = (int)p;
+            t.mi[(size_t)n * N + s] = M.add(mix + ((size_t)s * zm + n) * 24);
+        }
+    }
 }
 
 int method_mode(int method) {
@@ -107,26 +141,53 @@ int64_t loop_steps(double T0, double T1, double dt, std::vector<double>* grid) {
 }
 
 template <int CS>
-int launch_cs(cmd_mixed* h, const cmd::MixedRun& r, int threads) {
-    auto kern = cmd::mixed_integrate_kernel<CS>;
+cudaLaunchConfig_t config(cmd_mixed* h, int threads, cudaLaunchAttribute* attr) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(CS);
     cfg.blockDim = dim3((unsigned)threads);
-    cfg.dynamicSmemBytes = 0;
+    cfg.dynamicSmemBytes = h->m.tab_in_smem ? (size_t)h->m.tab_doubles * sizeof(double) : 0;
     cfg.stream = h->stream;
-    cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = CS;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    MIX_TRY(cudaLaunchKernelEx(&cfg, kern, h->m, r));
+    return cfg;
+}
+
+template <int CS>
+int set_attributes() {
+    static bool done = false;
+    if (!done) {
+        auto kern = cmd::mixed_integrate_kernel<CS>;
+        MIX_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMixedSmemMax));
+        if (CS > 8) MIX_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        done = true;
+    }
     return CMD_OK;
 }
 
+template <int CS>
+int launch_cs(cmd_mixed* h, const cmd::MixedRun& r, int threads) {
+    if (int rc = set_attributes<CS>()) return rc;
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = config<CS>(h, threads, attr);
+    MIX_TRY(cudaLaunchKernelEx(&cfg, cmd::mixed_integrate_kernel<CS>, h->m, r));
+    return CMD_OK;
+}
+
+// Whether a 16-CTA cluster (a non-portable size) of this shape can be resident.
+bool cluster16_fits(cmd_mixed* h, int threads) {
+    if (set_attributes<16>() != CMD_OK) return false;
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = config<16>(h, threads, attr);
+    int n = 0;
+    return cudaOccupancyMaxActiveClusters(&n, cmd::mixed_integrate_kernel<16>, &cfg) == cudaSuccess && n >= 1;
+}
+
 // One persistent launch over a cluster sized to the lattice: one site per thread up
-// to 8 CTAs of kMixedThreads, the threads loop beyond that.
+// to 16 CTAs, the threads loop beyond that (at most kMixedThreads per CTA).
 int run(cmd_mixed* h, int method, double T0, double dt, int64_t n_steps, int64_t save_every, int64_t max_rows) {
     const int mode = method_mode(method);
     if (mode < 0) return fail(CMD_ERR_INVALID_ARG, "the mixed path takes a fixed-step method (any CMD_* but CMD_RK45)");
@@ -144,14 +205,21 @@ int run(cmd_mixed* h, int method, double T0, double dt, int64_t n_steps, int64_t
     r.n_steps = n_steps;
     r.save_every = save_every;
     r.mode = mode;
+    // Up to 128 sites per CTA before the cluster grows (more SMs per trajectory beat
+    // more warps per SM here: the stages are latency-bound), up to 16 CTAs.
     const int64_t sites = (int64_t)h->m.N2 + h->m.N3;
-    const int64_t per = (sites + cmd::kMixedThreads - 1) / cmd::kMixedThreads;
-    const int cs = per <= 1 ? 1 : per <= 2 ? 2 : per <= 4 ? 4 : 8;
-    const int threads = (int)std::min<int64_t>(cmd::kMixedThreads, std::max<int64_t>(32, ((sites + cs - 1) / cs + 31) / 32 * 32));
+    const int64_t per = (sites + 127) / 128;
+    int cs = per <= 1 ? 1 : per <= 2 ? 2 : per <= 4 ? 4 : per <= 8 ? 8 : 16;
+    auto threads_for = [&](int c) {
+        return (int)std::min<int64_t>(cmd::kMixedThreads, std::max<int64_t>(32, ((sites + c - 1) / c + 31) / 32 * 32));
+    };
+    if (cs == 16 && !cluster16_fits(h, threads_for(16))) cs = 8;
+    const int threads = threads_for(cs);
     int rc = cs == 1 ? launch_cs<1>(h, r, threads)
            : cs == 2 ? launch_cs<2>(h, r, threads)
            : cs == 4 ? launch_cs<4>(h, r, threads)
-                     : launch_cs<8>(h, r, threads);
+           : cs == 8 ? launch_cs<8>(h, r, threads)
+                     : launch_cs<16>(h, r, threads);
     if (rc) return rc;
     MIX_TRY(cudaGetLastError());
     return CMD_OK;
@@ -197,47 +265,66 @@ int cmd_mixed_create(const cmd_mixed_desc* d, cmd_mixed** out) {
     };
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(fail(CMD_ERR_CUDA, "no CUDA device (cudaStreamCreate failed)"));
-    const std::vector<int> p2 = partners(d->partners_su2, (size_t)(N2 * z2), N2), c2 = counts(d->counts_su2, N2);
-    const std::vector<int> p3 = partners(d->partners_su3, (size_t)(N3 * z3), N3), c3 = counts(d->counts_su3, N3);
-    const std::vector<int> mp2 = partners(d->mixed_partners_su3, (size_t)(N2 * zm2), N3);
-    const std::vector<int> mc2 = counts(zm2 > 0 ? d->mixed_counts_su2 : nullptr, N2);
-    const std::vector<int> mp3 = partners(d->mixed_partners_su2, (size_t)(N3 * zm3), N2);
-    const std::vector<int> mc3 = counts(zm3 > 0 ? d->mixed_counts_su3 : nullptr, N3);
-    const size_t b_f2 = N2 * 3 * 8, b_o2 = N2 * 9 * 8, b_j2 = N2 * z2 * 9 * 8, b_m2 = N2 * zm2 * 24 * 8;
-    const size_t b_f3 = N3 * 8 * 8, b_o3 = N3 * 64 * 8, b_j3 = N3 * z3 * 64 * 8, b_m3 = N3 * zm3 * 24 * 8;
-    const size_t total = pad(b_f2) + pad(b_o2) + pad(b_j2) + pad(b_m2) + pad(b_f3) + pad(b_o3) + pad(b_j3) +
-                         pad(b_m3) + pad(p2.size() * 4) + pad(c2.size() * 4) + pad(mp2.size() * 4) +
-                         pad(mc2.size() * 4) + pad(p3.size() * 4) + pad(c3.size() * 4) + pad(mp3.size() * 4) +
-                         pad(mc3.size() * 4);
+    Distinct F2(3), O2(9), B2(9), M2(24), F3(8), O3(64), B3(64), M3(24);
+    KindTables k2, k3;
+    build_kind(N2, z2, zm2, 3, d->field_su2, d->onsite_su2, d->bilinear_su2, d->partners_su2, d->counts_su2, N2,
+               d->mixed_su2, d->mixed_partners_su3, d->mixed_counts_su2, N3, F2, O2, B2, M2, k2);
+    build_kind(N3, z3, zm3, 8, d->field_su3, d->onsite_su3, d->bilinear_su3, d->partners_su3, d->counts_su3, N3,
+               d->mixed_su3, d->mixed_partners_su2, d->mixed_counts_su3, N2, F3, O3, B3, M3, k3);
+    std::vector<double> tab;
+    cmd::MixedDev& m = h->m;
+    // each distinct block at the kernel's odd stride (mixed.cuh kStride*)
+    auto append = [&](const Distinct& D, int stride, int& off) {
+        off = (int)tab.size();
+        const size_t nb = D.vals.size() / D.w;
+        tab.resize(tab.size() + nb * stride, 0.0);
+        for (size_t b = 0; b < nb; ++b)
+            std::copy(D.vals.begin() + b * D.w, D.vals.begin() + (b + 1) * D.w, tab.begin() + off + b * stride);
+    };
+    append(F2, cmd::kStrideF2, m.off_f2); append(O2, cmd::kStrideO2, m.off_o2);
+    append(B2, cmd::kStrideB2, m.off_b2); append(M2, cmd::kStrideM, m.off_m2);
+    append(F3, cmd::kStrideF3, m.off_f3); append(O3, cmd::kStrideO3, m.off_o3);
+    append(B3, cmd::kStrideB3, m.off_b3); append(M3, cmd::kStrideM, m.off_m3);
+    // work slots: warp-sized runs of SU(2) and SU(3) sites in turn, so every CTA gets both kinds
+    std::vector<int> order;
+    order.reserve(N2 + N3);
+    for (int64_t a = 0, b = 0; a < N2 || b < N3;) {
+        for (int k = 0; k < 32 && a < N2; ++k) order.push_back((int)a++);
+        for (int k = 0; k < 32 && b < N3; ++k) order.push_back((int)(N2 + b++));
+    }
+    const std::vector<int>* ints[17] = {&k2.fi, &k2.oi, &k2.bi, &k2.part, &k2.cnt, &k2.mi, &k2.mpart, &k2.mcnt,
+                                        &k3.fi, &k3.oi, &k3.bi, &k3.part, &k3.cnt, &k3.mi, &k3.mpart, &k3.mcnt,
+                                        &order};
+    size_t total = pad(tab.size() * sizeof(double));
+    for (const auto* v : ints) total += pad(v->size() * sizeof(int));
     if (int rc = h->tables.ensure(total)) return bail(rc);
     char* cur = h->tables.as<char>();
-    cmd::MixedDev& m = h->m;
-    m.N2 = (int)N2; m.N3 = (int)N3;
-    m.NA2 = std::max(1, d->n_atoms_su2); m.NA3 = std::max(1, d->n_atoms_su3);
-    m.z2 = z2; m.z3 = z3; m.zm2 = zm2; m.zm3 = zm3;
     int rc = CMD_OK;
     auto put = [&](const void* src, size_t bytes) {
         char* at = cur;
-        if (rc == CMD_OK) rc = upload(h, src, bytes, cur);
+        if (rc == CMD_OK && bytes) {
+            if (cudaMemcpyAsync(cur, src, bytes, cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
+                rc = fail(CMD_ERR_CUDA, "upload of the mixed lattice tables failed");
+        }
+        cur += pad(bytes);
         return at;
     };
-    m.field2 = (const double*)put(d->field_su2, b_f2);
-    m.onsite2 = (const double*)put(d->onsite_su2, b_o2);
-    m.bil2 = (const double*)put(d->bilinear_su2, b_j2);
-    m.mix2 = (const double*)put(d->mixed_su2, b_m2);
-    m.field3 = (const double*)put(d->field_su3, b_f3);
-    m.onsite3 = (const double*)put(d->onsite_su3, b_o3);
-    m.bil3 = (const double*)put(d->bilinear_su3, b_j3);
-    m.mix3 = (const double*)put(d->mixed_su3, b_m3);
-    m.part2 = (const int*)put(p2.data(), p2.size() * 4);
-    m.cnt2 = (const int*)put(c2.data(), c2.size() * 4);
-    m.mpart2 = (const int*)put(mp2.data(), mp2.size() * 4);
-    m.mcnt2 = (const int*)put(mc2.data(), mc2.size() * 4);
-    m.part3 = (const int*)put(p3.data(), p3.size() * 4);
-    m.cnt3 = (const int*)put(c3.data(), c3.size() * 4);
-    m.mpart3 = (const int*)put(mp3.data(), mp3.size() * 4);
-    m.mcnt3 = (const int*)put(mc3.data(), mc3.size() * 4);
+    m.N2 = (int)N2; m.N3 = (int)N3;
+    m.NA2 = std::max(1, d->n_atoms_su2); m.NA3 = std::max(1, d->n_atoms_su3);
+    m.z2 = z2; m.z3 = z3; m.zm2 = zm2; m.zm3 = zm3;
+    m.tab = (const double*)put(tab.data(), tab.size() * sizeof(double));
+    m.tab_doubles = (int)tab.size();
+    m.tab_in_smem = tab.size() * sizeof(double) <= kMixedSmemMax;
+    const int* dev[17];
+    for (int i = 0; i < 17; ++i) dev[i] = (const int*)put(ints[i]->data(), ints[i]->size() * sizeof(int));
+    m.order = dev[16];
+    m.f2i = dev[0]; m.o2i = dev[1]; m.b2i = dev[2]; m.part2 = dev[3]; m.cnt2 = dev[4]; m.m2i = dev[5];
+    m.mpart2 = dev[6]; m.mcnt2 = dev[7];
+    m.f3i = dev[8]; m.o3i = dev[9]; m.b3i = dev[10]; m.part3 = dev[11]; m.cnt3 = dev[12]; m.m3i = dev[13];
+    m.mpart3 = dev[14]; m.mcnt3 = dev[15];
     if (rc) return bail(rc);
+    // the host vectors above must outlive the copies
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bail(fail(CMD_ERR_CUDA, "upload failed"));
     // drives start at zero, width 1 (the reference's defaults)
     const size_t bd2 = 2 * (size_t)m.NA2 * 3 * 8, bd3 = 2 * (size_t)m.NA3 * 8 * 8;
     if ((rc = h->drive2.ensure(bd2)) || (rc = h->drive3.ensure(bd3))) return bail(rc);

@@ -2,9 +2,9 @@
 restatement and against the reference's own mixed GPU code (oracle/_ref/libref_mixed.so).
 
 Tolerances: states <= 1e-12 after 20 steps (the two sides sum the same terms in another order);
-magnetisations <= 1e-14.  Lattices: seeded TmFeO3-shaped synthetic lattices, 2x2x2 cells (one CTA),
-6x6x6 (1728 sites: a 4-CTA cluster) and 10x10x10 (8000 sites: an 8-CTA cluster, two sites per thread),
-with a two-pulse drive on both kinds of site."""
+magnetisations <= 1e-14.  Lattices: seeded TmFeO3-shaped synthetic lattices of 8 sites per cell with a
+two-pulse drive on both kinds of site: 2x2x2 cells (one CTA), 3^3, 4^3, 5^3 and 6^3 cells (clusters of
+2, 4, 8 and 16 CTAs) and 12^3 (13824 sites on 16 CTAs of 512 threads: two sites per thread)."""
 import numpy as np
 import pytest
 
@@ -88,7 +88,7 @@ def test_mixed_matches_reference_gpu(mg, mo, oracle, method):
     assert np.abs(mg.get_gpu_mixed_spins(h) - rn).max() <= 1e-14
 
 
-@pytest.mark.parametrize("L", [(6, 6, 6), (10, 10, 10)])
+@pytest.mark.parametrize("L", [(3, 3, 3), (4, 4, 4), (5, 5, 5), (6, 6, 6), (12, 12, 12)])
 def test_mixed_cluster_sizes_match_oracle(mg, mo, L):
     import fixed_methods as fm
     arr, h, o = _setup(mg, mo, L, 15)

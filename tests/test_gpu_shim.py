@@ -97,3 +97,42 @@ def test_shim_call_sequence(native, oracle, tmp_path):
     ref.close()
     np.testing.assert_array_equal(_load(d, "batched_times"), bt)
     assert np.abs(_load(d, "batched_mags").reshape(bm.shape) - bm).max() <= 1e-12
+
+
+def test_mixed_shim_call_sequence(native, oracle, tmp_path):
+    """The mixed_gpu:: call sequence through include/classical_spin/gpu/mixed_lattice_gpu_api.h: bit-identical
+    to the Python mirror (same library); no-ops, dims and the unknown-method fall-back as in the reference."""
+    from classical_mcmc_spin_b200 import mixed_gpu_api as mg
+    exe = build_shim_program(tmp_path / "mixed_shim_calls", "mixed_shim_calls.cpp")
+    arr = mg.synthetic_mixed_lattice((2, 2, 3), seed=21)
+    y0 = mg.random_mixed_state(arr, 22)
+    rng = np.random.default_rng(23)
+    d2, d3 = rng.normal(size=2 * arr["na2"] * 3), rng.normal(size=2 * arr["na3"] * 8)
+    d = tmp_path / "io"
+    d.mkdir()
+    (d / "meta.txt").write_text(" ".join(str(arr[k]) for k in ("n2", "na2", "n3", "na3", "z2", "z3", "zm2", "zm3")))
+    for k in ("field2", "onsite2", "bil2", "field3", "onsite3", "bil3", "mix2", "mix3"):
+        np.ascontiguousarray(arr[k], dtype=np.float64).tofile(d / f"{k}.bin")
+    for k in ("part2", "cnt2", "part3", "cnt3", "mpart2", "mcnt2", "mpart3", "mcnt3"):
+        np.ascontiguousarray(arr[k], dtype=np.uint64).tofile(d / f"{k}.bin")
+    for k, v in (("spins", y0), ("drive2", d2), ("drive3", d3)):
+        np.ascontiguousarray(v, dtype=np.float64).tofile(d / f"{k}.bin")
+    r = subprocess.run([str(exe), str(d)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "Unknown GPU integration method 'no_such_method', using ssprk53" in r.stderr
+    np.testing.assert_array_equal(_load(d, "noop"), [1.0, 0.0, 0.0, arr["n2"], 3, arr["na2"], arr["n3"], 8,
+                                                     arr["na3"]])
+    h = mg.create_from(arr)
+    mg.set_gpu_pulse_SU2(h, d2, 0.6, 0.3, 1.2, 0.05, 0.25)
+    mg.set_gpu_pulse_SU3(h, d3, 0.4, 0.2, 0.8, 0.1, 0.3)
+    mg.set_gpu_mixed_spins(h, y0)
+    traj, times = mg.integrate_mixed_gpu(h, 0.0, 0.4, 0.02, 5)
+    np.testing.assert_array_equal(_load(d, "traj_times"), times)
+    np.testing.assert_array_equal(_load(d, "traj_states").reshape(len(times), -1), np.stack([s for _, s in traj]))
+    mg.step_mixed_gpu(h, 0.4, 0.02, "rk4")
+    np.testing.assert_array_equal(_load(d, "step_rk4"), mg.get_gpu_mixed_spins(h))
+    mg.step_mixed_gpu(h, 0.42, 0.02, "ssprk53")
+    np.testing.assert_array_equal(_load(d, "step_fallback"), mg.get_gpu_mixed_spins(h))
+    np.testing.assert_array_equal(_load(d, "mags"), np.concatenate(mg.compute_magnetization_mixed_gpu(h)))
+    mg.normalize_spins_mixed_gpu(h, 1.5, 0.7)
+    np.testing.assert_array_equal(_load(d, "normalized"), mg.get_gpu_mixed_spins(h))
