@@ -172,3 +172,38 @@ def test_mixed_faster_than_reference_gpu(mg, mo, capsys):
         print(f"\nmixed 6x6x6 RK4: reference {t_ref / (4 * S) * 1e6:.1f} us/stage, "
               f"B200 {t_b200 / (4 * S) * 1e6:.1f} us/stage, {t_ref / t_b200:.1f}x")
     assert t_ref >= 3.0 * t_b200
+
+
+def test_mixed_ragged_tables_match_reference_gpu(mg, mo):
+    """Ragged ELL tables: per-site counts below the width and partners outside the lattice (the reference
+    skips them, mixed_lattice_gpu.cu:92-118, 157-185); the unused slots hold garbage matrices, which must not
+    enter.  Against the reference's own code and the oracle."""
+    import fixed_methods as fm
+    if not (mo.REF_DIR / "libref_mixed.so").exists():
+        pytest.skip("oracle/_ref/libref_mixed.so not built")
+    arr = mg.synthetic_mixed_lattice((2, 2, 2), seed=40)
+    rng = np.random.default_rng(41)
+    for kp, kc, kv, z, n, limit, w in (("part2", "cnt2", "bil2", arr["z2"], arr["n2"], arr["n2"], 9),
+                                       ("part3", "cnt3", "bil3", arr["z3"], arr["n3"], arr["n3"], 64),
+                                       ("mpart2", "mcnt2", "mix2", arr["zm2"], arr["n2"], arr["n3"], 24),
+                                       ("mpart3", "mcnt3", "mix3", arr["zm3"], arr["n3"], arr["n2"], 24)):
+        cnt = rng.integers(0, z + 1, size=n)
+        part = arr[kp].reshape(n, z).copy()
+        part[rng.random((n, z)) < 0.2] = limit + rng.integers(0, 5)     # outside the lattice
+        val = arr[kv].reshape(n, z, w).copy()
+        for s in range(n):
+            val[s, cnt[s]:] = rng.normal(size=(z - cnt[s], w)) * 100     # never read
+        arr[kc], arr[kp], arr[kv] = cnt.astype(np.int64), part.ravel(), val.ravel()
+    y0 = mg.random_mixed_state(arr, 42)
+    h = mg.create_from(arr)
+    mg.set_gpu_mixed_spins(h, y0)
+    traj, times = mg.integrate_mixed_gpu(h, 0.0, 0.2, 0.02, 5, "rk4")
+    ref = mo.RefMixedGPU(arr)
+    ref.set_spins(y0)
+    rt, rs = ref.integrate(0.0, 0.2, 0.02, 5, "rk4")
+    ref.close()
+    np.testing.assert_array_equal(times, rt)
+    assert np.abs(np.stack([s for _, s in traj]) - rs).max() <= 1e-12
+    o = mo.MixedOracle(arr)
+    _, os_ = fm.integrate(lambda y, t: o.rhs(y, t), y0, 0.0, 0.2, 0.02, 5, "rk4")
+    assert np.abs(np.stack([s for _, s in traj]) - os_).max() <= 1e-12
