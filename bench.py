@@ -344,7 +344,10 @@ def leg_pyrochlore(torch, dev, S=20000, S_adj=2000):
     N, B, dt = lat.lattice_size, 32, 0.005
     h = lat.to_gpu()
     states = np.stack([random_unit_spins(N, 5000 + b).ravel() for b in range(B)])
+    clk = ClockSampler(dev.index if dev.index is not None else 0)
+    clk.start()
     fwd = _forward_device(torch, dev, h, states, S, dt, streamed=True)
+    fwd["clocks"] = clk.stop()
     h.close()
     adj = _adjoint_leg(torch, dev, build, theta, np.array([1.0, 0.06, 0.03, 0.25]), 4, B, S_adj, dt, 5,
                        int(np.ceil(np.sqrt(S_adj))))
