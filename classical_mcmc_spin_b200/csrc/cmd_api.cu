@@ -68,29 +68,7 @@ struct Layout {
     std::string why;            // reason when not uniform
 };
 
-struct DevBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
-    int ensure(size_t n) {
-        if (n <= bytes) return CMD_OK;
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-        cudaError_t e = cudaMalloc(&p, n);
-        if (e != cudaSuccess) {
-            p = nullptr;
-            return fail(CMD_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-        }
-        bytes = n;
-        return CMD_OK;
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-    }
-    template <class T> T* as() const { return static_cast<T*>(p); }
-};
+using cmd::DevBuf;
 
 }  // namespace
 

@@ -1,7 +1,11 @@
 // cmd_internal.h -- shared helpers of the C-ABI implementation (not installed).
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <string>
+
+#include "cmd.h"
 
 namespace cmd {
 
@@ -9,5 +13,30 @@ namespace cmd {
 int fail(int code, const std::string& msg);
 // Clears the last error (called at the start of every public entry point).
 void clear_error();
+
+// A device allocation that only grows; the owner calls release().
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t n) {
+        if (n <= bytes) return CMD_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return fail(CMD_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        }
+        bytes = n;
+        return CMD_OK;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
 
 }  // namespace cmd

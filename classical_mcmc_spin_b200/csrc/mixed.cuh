@@ -225,7 +225,6 @@ template <int CS>
 __global__ void __launch_bounds__(kMixedThreads, 1)
 mixed_integrate_kernel(const __grid_constant__ MixedDev m, const __grid_constant__ MixedRun r) {
     mcg::cluster_group cluster = mcg::this_cluster();
-    __shared__ double fs[4];
     extern __shared__ double stab[];       // the distinct couplings, when they fit
     const int nt = (int)blockDim.x * CS;
     const int gt = (int)cluster.block_rank() * (int)blockDim.x + (int)threadIdx.x;
@@ -241,20 +240,19 @@ mixed_integrate_kernel(const __grid_constant__ MixedDev m, const __grid_constant
     double* yn = r.work + 10 * V;
 
     const double* T = m.tab_in_smem ? stab : m.tab;
-    // every rhs call is preceded by a cluster barrier, so fs is free to rewrite
+    // drive factors of the stage time: lanes 0-3 of every warp compute one each and the
+    // warp shares them (no CTA barrier)
     auto rhs = [&](const double* Yin, double* K, double ts) {
+        double f[4] = {0.0, 0.0, 0.0, 0.0};
         if (driven) {
-            if (threadIdx.x < 4) {
-                const int q = threadIdx.x;
-                fs[q] = q == 0   ? drive_factor(m.amp2, ts - m.t1_2, m.width2, m.freq2)
-                        : q == 1 ? drive_factor(m.amp2, ts - m.t2_2, m.width2, m.freq2)
-                        : q == 2 ? drive_factor(m.amp3, ts - m.t1_3, m.width3, m.freq3)
-                                 : drive_factor(m.amp3, ts - m.t2_3, m.width3, m.freq3);
-            }
-            __syncthreads();
+            const int q = threadIdx.x & 3;
+            const double v = q == 0   ? drive_factor(m.amp2, ts - m.t1_2, m.width2, m.freq2)
+                             : q == 1 ? drive_factor(m.amp2, ts - m.t2_2, m.width2, m.freq2)
+                             : q == 2 ? drive_factor(m.amp3, ts - m.t1_3, m.width3, m.freq3)
+                                      : drive_factor(m.amp3, ts - m.t2_3, m.width3, m.freq3);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) f[k] = __shfl_sync(0xffffffffu, v, k);
         }
-        const double f[4] = {driven ? fs[0] : 0.0, driven ? fs[1] : 0.0, driven ? fs[2] : 0.0,
-                             driven ? fs[3] : 0.0};
         for (int q = gt; q < sites; q += nt) mixed_rhs_site(m, T, Yin, K, m.order[q], f);
     };
     // the elements of the thread's own sites: the ones its rhs writes (rk_fixed.cuh reads

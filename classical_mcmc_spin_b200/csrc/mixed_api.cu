@@ -16,44 +16,23 @@
 
 using cmd::fail;
 
-namespace {
-
 #define MIX_TRY(x)                                                                               \
     do {                                                                                         \
         cudaError_t e_ = (x);                                                                    \
         if (e_ != cudaSuccess) return fail(CMD_ERR_CUDA, std::string(#x ": ") + cudaGetErrorString(e_)); \
     } while (0)
 
-struct Buf {
-    void* p = nullptr;
-    size_t bytes = 0;
-    int ensure(size_t n) {
-        if (n <= bytes) return CMD_OK;
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-        if (cudaMalloc(&p, std::max<size_t>(n, 8)) != cudaSuccess) {
-            p = nullptr;
-            return fail(CMD_ERR_OOM, "cudaMalloc failed for the mixed lattice");
-        }
-        bytes = n;
-        return CMD_OK;
-    }
-    template <class T>
-    T* as() const { return static_cast<T*>(p); }
-    ~Buf() { if (p) cudaFree(p); }
-};
-
-}  // namespace
-
 struct cmd_mixed {
     cmd::MixedDev m{};
     int64_t V = 0;
-    Buf tables;                // all coupling tables, one allocation
-    Buf drive2, drive3;
-    Buf state, work, rows, mag;
+    cmd::DevBuf tables;        // distinct couplings and index arrays, one allocation
+    cmd::DevBuf drive2, drive3;
+    cmd::DevBuf state, work, rows, mag;
     bool has_state = false;
     cudaStream_t stream = nullptr;
+    ~cmd_mixed() {
+        for (cmd::DevBuf* b : {&tables, &drive2, &drive3, &state, &work, &rows, &mag}) b->release();
+    }
 };
 
 namespace {
