@@ -1602,6 +1602,12 @@ void fill_param_derivs(const std::vector<double>& DJ, const std::vector<double>&
             std::memcpy(pd.DA[q][at], &DA[((size_t)q * NAT + at) * 9], 9 * sizeof(double));
         }
     pd.has_DA = has_DA;
+    for (int q = 0; q < NQ; ++q) {
+        pd.dj_any[q] = 0;
+        for (int at = 0; at < NAT; ++at)
+            for (int s = 0; s < Z; ++s)
+                for (int e = 0; e < 9; ++e) pd.dj_any[q] |= pd.DJ[q][at][s][e] != 0.0;
+    }
 }
 
 template <int NAT, int Z, int LZ>

@@ -50,6 +50,7 @@ struct ParamDerivs {
     double DB[NQ][NAT][3];
     double DA[NQ][NAT][9];
     int has_DA;
+    int dj_any[NQ];            // parameter q has a non-zero coupling derivative (resident adjoint skips it if not)
 };
 
 struct AdjTraj {

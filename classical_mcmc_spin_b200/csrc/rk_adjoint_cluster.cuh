@@ -419,6 +419,7 @@ adjoint_cluster_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __gri
                             }
 #pragma unroll
                             for (int q = 0; q < NQ; ++q) {
+                                if (!pd.dj_any[q]) continue;        // e.g. a field parameter
                                 const double* D = pd.DJ[q][at][n_];
                                 gq[q] += S0 * (D[0] * Q[0] + D[1] * Q[1] + D[2] * Q[2]) +
                                          S1 * (D[3] * Q[0] + D[4] * Q[1] + D[5] * Q[2]) +
