@@ -48,24 +48,48 @@ L_SIDE = 24
 
 
 # --------------------------------------------------------------------------- workload
-def scan_workload(n_steps: int, rank: int = 0, world: int = 1):
-    from classical_mcmc_spin_b200.lattice import Lattice
-    from classical_mcmc_spin_b200.states import zigzag_honeycomb
+def zigzag_tilted(d1: int, d2: int, sigma: float, seed: int) -> np.ndarray:
+    """The scan's initial state in numpy alone (the reference arm never imports the package): site
+    (i, j, atom) of the 2-atom honeycomb gets (-1)^i (1,1,1)/sqrt3, tilted by i.i.d. Gaussian components of
+    width sigma (seed) and renormalised.  Equal to classical_mcmc_spin_b200.states.zigzag_honeycomb
+    (tests/test_bench_inputs.py checks it)."""
+    axis = np.ones(3) / np.sqrt(3.0)
+    i = np.arange(d1).repeat(d2 * 2)
+    s = np.where(i % 2 == 0, 1.0, -1.0)[:, None] * axis[None, :]
+    s = s + sigma * np.random.default_rng(seed).standard_normal(s.shape)
+    return s / np.linalg.norm(s, axis=1, keepdims=True)
 
-    lat = Lattice.kitaev(L_SIDE, L_SIDE, 1, K=-1.0, Gamma=0.25, Gammap=-0.02)
-    s0 = zigzag_honeycomb(L_SIDE, L_SIDE, 1, tilt_sigma=0.05, seed=2).ravel()
+
+def scan_inputs(n_steps: int, rank: int = 0, world: int = 1) -> dict:
+    """Inputs of the 2DCS scan (numpy only).  Weak scaling: rank r scans its interleaved share of a
+    world x 256 delay scan, tau = 100 (k + r / world) / 255."""
+    s0 = zigzag_tilted(L_SIDE, L_SIDE, 0.05, 2).ravel()
     fin = np.tile(np.ones(3) / np.sqrt(3.0), 2)
-    fd = lat.rotate_pulse(fin, fin)
-    # weak scaling: rank r scans its interleaved share of a world x 256 delay scan
-    from classical_mcmc_spin_b200.sharding import scan_delays
-    taus = scan_delays(N_DELAYS, 100.0, rank, world)
+    taus = 100.0 * (np.arange(N_DELAYS) + rank / world) / (N_DELAYS - 1)
     pulses = []
     for tau in taus:
         for a1, a2 in ((0.5, 0.0), (0.0, 0.5), (0.5, 0.5)):
             pulses.append((0.0, tau, a1, a2))
-    pulses = np.array(pulses)
-    return dict(lat=lat, s0=s0, fin=fin, d1=fd[:6].copy(), d2=fd[6:].copy(), pulses=pulses, T0=-5.0, dt=0.01,
-                n_steps=n_steps, width=0.5, freq=0.0)
+    return dict(s0=s0, fin=fin, pulses=np.array(pulses), T0=-5.0, dt=0.01, n_steps=n_steps, width=0.5, freq=0.0)
+
+
+def scan_workload(n_steps: int, rank: int = 0, world: int = 1):
+    from classical_mcmc_spin_b200.lattice import Lattice
+
+    wl = scan_inputs(n_steps, rank, world)
+    lat = Lattice.kitaev(L_SIDE, L_SIDE, 1, K=-1.0, Gamma=0.25, Gammap=-0.02)
+    fd = lat.rotate_pulse(wl["fin"], wl["fin"])
+    wl.update(lat=lat, d1=fd[:6].copy(), d2=fd[6:].copy())
+    return wl
+
+
+def scan_config(n_steps: int, world: int) -> dict:
+    """`config` of the headline line, identical in both arms."""
+    return {"workload": "2dcs_scan_kitaev24x24_768traj_rk4", "spins": 2 * L_SIDE * L_SIDE,
+            "trajectories": 3 * N_DELAYS, "rk4_steps": n_steps, "dt": 0.01, "T_start": -5.0, "delays": N_DELAYS,
+            "observables_every_step": True, "energy_every_step": True,
+            "l2": "flushed between timed iterations (256 MB write)",
+            "parallelism": f"replicas: {world} GPU(s), trajectories sharded, no collective"}
 
 
 # --------------------------------------------------------------------------- clocks
@@ -356,15 +380,23 @@ def leg_pyrochlore(torch, dev, S=20000, S_adj=2000):
 
 
 # --------------------------------------------------------------------------- CPU baseline
-def cpu_baseline(wl, target_s: float = 8.0):
+def _oracle():
     sys.path.insert(0, str(ROOT / "oracle"))
     import ll_oracle as O
-    threads = os.cpu_count() or 1
+    return O
+
+
+def cpu_baseline(wl, target_s: float = 8.0, threads: int = 0):
+    """The oracle (CPU restatement of the reference's landau_lifshitz_flat + RK4, OpenMP) on a bounded sample
+    of the scan: max(threads, 8) trajectories spread over the delays, one per thread (the reference's W2 delay
+    loop, lattice_md.cpp:809-904), observables and energy every step as on the GPU."""
+    O = _oracle()
+    threads = threads or (os.cpu_count() or 1)
     O.set_threads(threads)
     lat = O.OracleLattice.kitaev(L_SIDE, L_SIDE, 1, K=-1.0, Gamma=0.25, Gammap=-0.02)
     N = lat.N
     P = wl["pulses"]
-    pick = np.linspace(0, len(P) - 1, max(threads, 8)).astype(int)
+    pick = np.linspace(0, len(P) - 1, max(threads, 8) if threads > 1 else 1).astype(int)
     B = len(pick)
     s = np.tile(wl["s0"], (B, 1))
     sub = P[pick]
@@ -374,7 +406,7 @@ def cpu_baseline(wl, target_s: float = 8.0):
     def run(steps):
         t0 = time.perf_counter()
         lat.batch_rk4(s, sub[:, 0], sub[:, 1], s1, s2, 0.5, wl["width"], wl["freq"], wl["fin"], wl["fin"], wl["T0"],
-                      wl["dt"], steps, with_obs=True, with_energy=False)
+                      wl["dt"], steps, with_obs=True, with_energy=True)
         return time.perf_counter() - t0
 
     probe = 20
@@ -382,17 +414,61 @@ def cpu_baseline(wl, target_s: float = 8.0):
     steps = int(max(20, min(20000, probe * target_s / max(tp, 1e-6))))
     wall = run(steps)
     return dict(value=B * N * steps / wall, unit=UNIT, cores=threads, kind="port",
-                sample=f"{B} of the 768 scan trajectories x {steps} RK4 steps (1152 spins, observables every step), "
-                       f"oracle restatement of the reference CPU RHS + RK4, trajectory-parallel OpenMP, "
-                       f"{wall:.2f} s wall"), (B, steps, wall)
+                sample=f"{B} of the 768 scan trajectories x {steps} RK4 steps (1152 spins, M and E every step), "
+                       f"oracle restatement of the reference CPU RHS + RK4, "
+                       f"{'trajectory-parallel OpenMP' if threads > 1 else 'one thread'}, {wall:.2f} s wall"), \
+        (B, steps, wall)
+
+
+def cpu_calibration(threads: int, n_rhs: int = 4000, repeats: int = 3) -> dict:
+    """bench_md-style row (src/apps/bench_md.cpp:214-231, 365-385): RHS calls/s of the oracle's
+    landau_lifshitz_flat restatement (site-parallel OpenMP) on the Kitaev honeycomb L = 32 (2048 spins, K=-1,
+    Gamma=0.25, Gamma'=-0.02, no field), warm-up max(500, n/4) calls, best of `repeats`; for comparison with
+    the reference's published 1.64e4 rhs/s (1 thread) ... 1.04e5 (16 threads) on its own host."""
+    O = _oracle()
+    O.set_threads(threads)
+    lat = O.OracleLattice.kitaev(32, 32, 1, K=-1.0, Gamma=0.25, Gammap=-0.02)
+    rng = np.random.default_rng(7)
+    x = rng.standard_normal((lat.N, 3))
+    x = (x / np.linalg.norm(x, axis=1, keepdims=True)).ravel()
+    out = np.zeros_like(x)
+    f = O.lib().ora_rhs
+    xp, op = O._p(x), O._p(out)
+
+    def run(n):
+        t = 0.0
+        for _ in range(n):
+            f(lat.h, xp, t, op)
+            t += 1e-3
+
+    run(max(500, n_rhs // 4))
+    best = 0.0
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        run(n_rhs)
+        best = max(best, n_rhs / (time.perf_counter() - t0))
+    return {"rhs_per_s": best, "threads": threads, "spins": lat.N,
+            "spin_rk4_steps_per_s": best * lat.N / 4.0,
+            "workload": "bench_md lattice row: kitaev-honeycomb-su2 L=32, oracle landau_lifshitz_flat restatement"}
+
+
+def cpu_rows(wl, target_s: float) -> dict:
+    """The CPU figures printed beside the baseline: the scan sample on one thread and the bench_md-style
+    calibration rows on one thread and on every host thread."""
+    n = os.cpu_count() or 1
+    one, _ = cpu_baseline(wl, target_s=max(2.0, target_s / 2), threads=1)
+    return {"one_thread": one, "calibration": [cpu_calibration(1), cpu_calibration(n)]}
 
 
 # --------------------------------------------------------------------------- reference arm
 def run_reference(args):
+    """The reference's CPU path on the host cores: the oracle port (the reference's own CPU build needs
+    Eigen3 / Boost / HDF5 / MPI, absent here).  Inputs come from numpy alone; this arm never imports the
+    package or loads its library."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    wl = scan_workload(args.md_steps)
+    wl = scan_inputs(args.md_steps)
     results = []
     for i in range(args.warmup + args.steps):
         base, (B, steps, wall) = cpu_baseline(wl, target_s=args.cpu_seconds)
@@ -405,13 +481,14 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * statistics.median([r[1] for r in results]), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "2dcs_scan_kitaev24x24_768traj_rk4", "sample_trajectories": B,
-                       "sample_steps": steps, "spins": L_SIDE * L_SIDE * 2},
+            "config": scan_config(args.md_steps, args.gpus),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-                             "sample": f"{B} scan trajectories x {steps} RK4 steps per bench step; the reference's "
-                                       "own CPU build needs Eigen3/Boost/HDF5/MPI (absent), so the oracle "
-                                       "restatement of its CPU integrator is timed"},
+                             "sample": f"{B} scan trajectories x {steps} RK4 steps per bench step, M and E every "
+                                       "step; the reference's own CPU build needs Eigen3/Boost/HDF5/MPI (absent), "
+                                       "so the oracle restatement of its CPU integrator is timed"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_cpu_rows:
+        line["cpu_rows"] = cpu_rows(wl, args.cpu_seconds)
     print(json.dumps(line), flush=True)
     return 0
 
@@ -428,6 +505,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
+    ap.add_argument("--no-cpu-rows", action="store_true", help="skip the 1-thread and calibration CPU rows")
     ap.add_argument("--no-peak", action="store_true", help="skip the DGEMM peak probe (profiling runs)")
     ap.add_argument("--legs", default="uneven,adjoint,kitaev48,pyrochlore,mixed",
                     help="further workloads to time on rank 0 (comma list; empty for none)")
@@ -607,6 +685,8 @@ def main():
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu, _ = cpu_baseline(wl, target_s=args.cpu_seconds)
+    cpu_extra = cpu_rows(wl, args.cpu_seconds) if (rank == 0 and not args.no_cpu_baseline
+                                                   and not args.no_cpu_rows) else None
     legs = {}
     if rank == 0:
         want = [x for x in args.legs.split(",") if x]
@@ -625,11 +705,8 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": "2dcs_scan_kitaev24x24_768traj_rk4", "spins": N, "trajectories": B,
-                           "rk4_steps": S, "dt": wl["dt"], "T_start": wl["T0"], "delays": N_DELAYS,
-                           "observables_every_step": True, "l2": "flushed between timed iterations (256 MB write)",
-                           "parallelism": f"replicas: {world} GPU(s), trajectories sharded, no collective"},
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+                "config": scan_config(S, world),
+                "roofline": roofline, "cpu_baseline": cpu, "cpu_rows": cpu_extra, "e2e": e2e, "clocks": clocks,
                 "gpu_launches": n_launch, "plain_path": plain,
                 "batched_over_plain": (value / world) / plain["value"] if plain else None,
                 "adjoint_over_forward": legs["adjoint_kitaev48"]["ratio"] if "adjoint_kitaev48" in legs else None,

@@ -70,6 +70,30 @@ struct Layout {
 
 using cmd::DevBuf;
 
+// Scratch of the allocation-free entry point (cmd_run_batch_device_noalloc):
+// 2^22 doubles (32 MiB) per device.  The array is part of this file's device
+// module, so every GPU that loads the module (at cmd_create at the latest, see
+// noalloc_lookup) holds it until the process exits.  In host code
+// `g_noalloc_scratch` is only a stand-in for the symbol; its device address
+// comes from cudaGetSymbolAddress.
+constexpr int64_t kNoAllocScratchDoubles = (int64_t)1 << 22;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+
+// Device address of g_noalloc_scratch on the current device.  cmd_create calls
+// it with the handle's device current and keeps the address in the handle, so
+// the module (and the 32 MiB with it) is loaded at handle creation, never
+// inside an allocation-free call, and a handle created after a context
+// teardown looks the address up afresh.
+int noalloc_lookup(double** out) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+        return fail(e == cudaErrorMemoryAllocation ? CMD_ERR_OOM : CMD_ERR_CUDA,
+                    std::string("cudaGetSymbolAddress(allocation-free scratch): ") + cudaGetErrorString(e));
+    *out = static_cast<double*>(p);
+    return CMD_OK;
+}
+
 }  // namespace
 
 struct cmd_handle {
@@ -90,6 +114,8 @@ struct cmd_handle {
     DevBuf cnbr2, cnbr4;         // partner tables of the 2- and 4-CTA cluster kernels (built at create)
     cudaStream_t copy_stream = nullptr;  // cmd_run_batch: device-to-host copies of finished chunks
     bool has_state = false;
+    int device = -1;            // device current at cmd_create (owns the stream and buffers)
+    double* noalloc_base = nullptr;   // device address of the allocation-free scratch on `device`
     int variant = -1;           // resident-kernel variant; -1 = heuristic default
     // pulse (set_gpu_pulse)
     std::vector<double> fd;     // [2][NA*3]
@@ -306,11 +332,10 @@ int launch_one(const cmd_handle* h, const cmd::ResidentArgs& args, const double*
     if (threads > MAXT) return fail(CMD_ERR_UNSUPPORTED, "lattice too large for this kernel variant");
     const size_t smem = resident_smem(NAT, G, TPC);
     if (smem > kMaxSmem) return fail(CMD_ERR_UNSUPPORTED, "stage buffers exceed shared memory");
-    static bool attr_set = false;
-    if (!attr_set) {
-        CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
-        attr_set = true;
-    }
+    // Function attributes belong to the current device's context: set on every
+    // launch (a host-side call of about a microsecond), so handles on several
+    // devices, several host threads and a re-created context all see it.
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
     cmd::Couplings<NAT, Z> cp;
     fill_couplings<NAT, Z>(h, d1, d2, cp);
     cmd::ResidentArgs a = args;
@@ -359,11 +384,10 @@ int launch_cluster(const cmd_handle* h, const cmd::ResidentArgs& args, const dou
     if (smem > kMaxSmem) return fail(CMD_ERR_UNSUPPORTED, "stage buffers exceed shared memory");
     const DevBuf& tab = CS == 2 ? h->cnbr2 : h->cnbr4;
     if (!tab.p) return fail(CMD_ERR_UNSUPPORTED, "no cluster neighbour table for this lattice");
-    static bool attr_set = false;
-    if (!attr_set) {
-        CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
-        attr_set = true;
-    }
+    // Function attributes belong to the current device's context: set on every
+    // launch (a host-side call of about a microsecond), so handles on several
+    // devices, several host threads and a re-created context all see it.
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
     cmd::Couplings<NAT, Z> cp;
     fill_couplings<NAT, Z>(h, d1, d2, cp);
     cmd::ResidentArgs a = args;
@@ -957,8 +981,11 @@ int cmd_create(const cmd_lattice_desc* d, cmd_handle** out) {
         h->n_atoms_ref = d->n_atoms;
     }
     int rc = CMD_OK;
-    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaGetDevice(&h->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
         rc = fail(CMD_ERR_CUDA, "cudaStreamCreate failed (no CUDA device?)");
+    } else if ((rc = noalloc_lookup(&h->noalloc_base)) != CMD_OK) {
+        // the device module (with the allocation-free scratch) could not be loaded
     } else if (h->lay.uniform) {
         rc = h->nbr.ensure(std::max<size_t>(h->lay.nbr.size(), 1) * sizeof(int));
         if (rc == CMD_OK && !h->lay.nbr.empty() &&
@@ -1645,11 +1672,10 @@ int launch_adjoint_cluster(cmd_handle* h, cmd::AdjClusterArgs a, const std::vect
     if (threads > MAXT || smem > kMaxSmem) return fail(CMD_ERR_UNSUPPORTED, "lattice too large for this adjoint variant");
     a.nbr = cluster_table(h, CS);
     if (!a.nbr && !h->lay.nbr.empty()) return fail(CMD_ERR_UNSUPPORTED, "no cluster neighbour table for this lattice");
-    static bool attr_set = false;
-    if (!attr_set) {
-        CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
-        attr_set = true;
-    }
+    // Function attributes belong to the current device's context: set on every
+    // launch (a host-side call of about a microsecond), so handles on several
+    // devices, several host threads and a re-created context all see it.
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
     cmd::Couplings<NAT, Z> cp;
     fill_couplings<NAT, Z>(h, h->fd.data(), h->fd.data() + 3 * h->NA, cp);
     cmd::ParamDerivs<NAT, Z, kAdjParams> pd;
@@ -2204,35 +2230,6 @@ int cmd_integrate_batched(cmd_handle* h, const double* init, const double* tau2,
 // kernels with that scratch carved out of one file-scope device array instead.
 namespace {
 
-// Scratch of the allocation-free entry point: 2^22 doubles (32 MiB) per
-// device, which every GPU that loads this library holds until the process
-// exits.  In host code `g_noalloc_scratch` is only a stand-in for the symbol;
-// its device address comes from cudaGetSymbolAddress.
-constexpr int64_t kNoAllocScratchDoubles = (int64_t)1 << 22;
-static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
-
-constexpr int kNoAllocMaxDevices = 64;
-std::mutex g_noalloc_mu;
-double* g_noalloc_base[kNoAllocMaxDevices] = {};
-
-// Device address of g_noalloc_scratch on the current device, looked up on the
-// first call per device (with that device current) and cached.
-int noalloc_scratch(double** out) {
-    int dev = -1;
-    CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(CMD_ERR_UNSUPPORTED, "device ordinal beyond 63");
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_base[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            return fail(CMD_ERR_CUDA, std::string("cudaGetSymbolAddress(noalloc scratch): ") + cudaGetErrorString(e));
-        g_noalloc_base[dev] = static_cast<double*>(p);
-    }
-    *out = g_noalloc_base[dev];
-    return CMD_OK;
-}
-
 // t_k of the reference loop (t = T0; t += dt) for k < n, by one thread: the
 // same sequence of IEEE additions as the host-built grid of run_resident.
 __global__ void time_grid_kernel(double T0, double dt, int64_t n, double* out) {
@@ -2252,7 +2249,12 @@ constexpr int64_t noalloc_round(int64_t n) { return (n + 31) / 32 * 32; }   // 2
 int run_resident_noalloc(cmd_handle* h, const RunSpec& r, cudaStream_t st, int32_t* launches) {
     int32_t nl = 0;
     const int vi = pick_variant(h);
-    if (vi < 0 || !variant_fits(kVariants[vi], h->lay)) return no_instance(h->lay);
+    if (vi < 0 || !variant_fits(kVariants[vi], h->lay)) {
+        if (!h->lay.uniform) return no_instance(h->lay);
+        return fail(CMD_ERR_UNSUPPORTED, "cmd_run_batch_device_noalloc runs resident lattices only (one CTA or a "
+                                         "2- or 4-CTA cluster per trajectory); this lattice needs the streamed "
+                                         "kernels: use cmd_run_batch_device");
+    }
     const Variant& V = kVariants[vi];
     if (r.n_steps > kNoAllocScratchDoubles)
         return fail(CMD_ERR_INVALID_ARG, "cmd_run_batch_device_noalloc: n_steps beyond the static scratch");
@@ -2274,8 +2276,12 @@ int run_resident_noalloc(cmd_handle* h, const RunSpec& r, cudaStream_t st, int32
                       (long long)kNoAllocScratchDoubles);
         return fail(CMD_ERR_INVALID_ARG, buf);
     }
-    double* base = nullptr;
-    if (int rc = noalloc_scratch(&base)) return rc;
+    int dev = -1;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev != h->device || !h->noalloc_base)
+        return fail(CMD_ERR_INVALID_ARG, "cmd_run_batch_device_noalloc: make the handle's device current (the "
+                                         "scratch address belongs to the device the handle was created on)");
+    double* base = h->noalloc_base;
     double* s_times = base;
     double* s_drive = base + n_times;
     double* s_raw = base + n_times + n_drive;
@@ -2340,7 +2346,8 @@ int cmd_run_batch_device_noalloc(cmd_handle* h, const cmd_batch_desc* d, void* s
     cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
     const bool drive = d->d1 || d->d2;
     if (drive && !d->pulse4) return fail(CMD_ERR_INVALID_ARG, "driven device batch needs pulse4");
-    if (h->NA > 64) return fail(CMD_ERR_UNSUPPORTED, "cmd_run_batch_device_noalloc: cells limited to 64 atoms");
+    if (drive && h->NA > 64)
+        return fail(CMD_ERR_UNSUPPORTED, "cmd_run_batch_device_noalloc: pulse directions limited to 64 atoms per cell");
     RunSpec r;
     r.B = d->B;
     r.y0 = d->states;

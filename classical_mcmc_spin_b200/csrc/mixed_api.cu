@@ -135,15 +135,14 @@ cudaLaunchConfig_t config(cmd_mixed* h, int threads, cudaLaunchAttribute* attr) 
     return cfg;
 }
 
+// Function attributes belong to the current device's context, so they are set
+// before every launch (a host-side call of about a microsecond): handles on
+// several devices, several host threads and a re-created context all see them.
 template <int CS>
 int set_attributes() {
-    static bool done = false;
-    if (!done) {
-        auto kern = cmd::mixed_integrate_kernel<CS>;
-        MIX_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMixedSmemMax));
-        if (CS > 8) MIX_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-        done = true;
-    }
+    auto kern = cmd::mixed_integrate_kernel<CS>;
+    MIX_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMixedSmemMax));
+    if (CS > 8) MIX_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     return CMD_OK;
 }
 

@@ -206,17 +206,21 @@ int cmd_run_batch_device(cmd_handle* h, const cmd_batch_desc* d, void* stream, i
  * memory already belongs to another allocator (a caching allocator that has
  * reserved the GPU, a pre-partitioned serving pool), or they run loops that
  * cannot take the device-wide synchronisation cudaMalloc / cudaFree may imply.
- * Same arguments and results as cmd_run_batch_device, and the same kernels.
+ * Same arguments and results as cmd_run_batch_device, for resident lattices
+ * only (those one CTA or a 2- or 4-CTA cluster holds: cmd_layout_info reports
+ * the path); a lattice that needs the streamed kernels is rejected with
+ * CMD_ERR_UNSUPPORTED, and cmd_run_batch_device runs it.
  * The scratch that cmd_run_batch_device allocates on demand lives here in one
- * static device array of 2^22 doubles (32 MiB), which every GPU that loads
- * this library holds until the process exits:
+ * static device array of 2^22 doubles (32 MiB).  It is part of the library's
+ * device module, which is loaded (and the 32 MiB taken) at cmd_create at the
+ * latest; every GPU that loads it holds it until the process exits:
  *     scratch doubles = [driven] n_steps + B*n_steps*6
  *                     + [cells of more than 3 atoms] B*rows*(3*atoms+1)
  * (each term rounded up to a multiple of 32).  A batch needing more is
  * rejected with CMD_ERR_INVALID_ARG; split it into smaller batches.
- * The call allocates no device memory.  Its first call on a device looks up
- * the array's device address (cudaGetSymbolAddress) with that device
- * current; make that first call before any stream capture.  Every call
+ * The call allocates no device memory: cmd_create looks up the array's device
+ * address (cudaGetSymbolAddress) with the handle's device current and keeps it
+ * in the handle, so call this with the handle's device current.  Every call
  * shares the one array, so calls whose work overlaps on the GPU (other
  * streams, other handles, other threads) race: order them on one stream, or
  * synchronise between them.  Everything a call reads from the array it first
