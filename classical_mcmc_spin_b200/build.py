@@ -10,6 +10,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -21,7 +22,8 @@ BUILD = PKG / "_build"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-O3"]
-SOURCES = ["cmd_api.cu", "mixed_api.cu", "spectrum.cu", "lattice_host.cpp"]
+SOURCES = ["cmd_api.cu", "resident.cu", "stream.cu", "global.cu", "adjoint.cu", "noalloc.cu", "mixed_api.cu",
+           "spectrum.cu", "lattice_host.cpp"]
 DRIVER = PKG / "cmd_spin_solver"          # command-line driver (csrc/spin_solver.cpp) over the C ABI
 
 
@@ -40,23 +42,40 @@ def _newer(target: Path, deps) -> bool:
 
 
 def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) -> Path:
-    deps = [CSRC / s for s in SOURCES] + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) \
-        + list((ROOT / "include").glob("*.h"))
+    """Compiles every source (in parallel, each object only when it is older than
+    its source or any header) and links libcmd_b200.so."""
+    headers = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list((ROOT / "include").glob("*.h"))
+    deps = [CSRC / s for s in SOURCES] + headers
     if not force and not ptxas_info and _newer(LIB, deps):
         build_driver(verbose, force)
         return LIB
     BUILD.mkdir(exist_ok=True)
-    objs = []
     inc = ["-I", str(ROOT / "include"), "-I", str(CSRC)]
+    jobs = []
     for src in SOURCES:
         obj = BUILD / (Path(src).stem + ".o")
+        if not force and not ptxas_info and _newer(obj, [CSRC / src] + headers):
+            continue
         cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *inc, "-c", str(CSRC / src), "-o", str(obj)]
         if ptxas_info and src.endswith(".cu"):
             cmd.insert(1, "-Xptxas=-v")
+        jobs.append(cmd)
+
+    def run(cmd):
         if verbose:
             print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
-        objs.append(str(obj))
+        return subprocess.run(cmd, capture_output=True, text=True)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(run, jobs))
+    failed = [r for r in results if r.returncode != 0]
+    for r in results:
+        if verbose or r.returncode != 0:
+            sys.stdout.write(r.stdout)
+            sys.stderr.write(r.stderr)
+    if failed:
+        raise RuntimeError(f"{len(failed)} source(s) failed to compile")
+    objs = [str(BUILD / (Path(src).stem + ".o")) for src in SOURCES]
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart", "-lcufft"]
     if verbose:

@@ -121,7 +121,7 @@ __device__ __forceinline__ void drive_acc(double& h, double d1, double d2, doubl
 
 // Envelope table [B][n_steps][6]: for each step n the factors (pulse 1, pulse 2)
 // at t_n, t_n + dt/2 and t_n + dt, t_n the accumulated time of the reference loop.
-__global__ void drive_table_kernel(const Pulse* __restrict__ pulses, const double* __restrict__ times,
+static __global__ void drive_table_kernel(const Pulse* __restrict__ pulses, const double* __restrict__ times,
                                    long long n_steps, double dt, double width, double freq, long long B,
                                    double* __restrict__ out) {
     const long long total = B * n_steps * 6;

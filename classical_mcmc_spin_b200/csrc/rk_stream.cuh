@@ -409,7 +409,7 @@ stream_vjp_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_con
 }
 
 // grad[b][q] = sum over tiles of the partials (tile order); one CTA per trajectory.
-__global__ void stream_grad_kernel(const double* __restrict__ gpart, int tiles, int nq, double* __restrict__ out,
+static __global__ void stream_grad_kernel(const double* __restrict__ gpart, int tiles, int nq, double* __restrict__ out,
                                    long long out_stride) {
     const int b = blockIdx.x;
     const int q = threadIdx.x;
