@@ -190,7 +190,9 @@ STREAM_BYTES_PER_SPIN_STEP = 408.0   # stages 72 + 120 + 120 + 96 B (input, y, R
 
 def leg_uneven(torch, dev, max_steps=10000, T1=100.0, B=512):
     """Uneven batch: 512 trajectories, honeycomb L in {8..32} and pyrochlore 16L^3, L in {4, 6, 8}, drawn from
-    seed 3; controlled RK45 at tol 1e-10, T_end = 100, cap 1e4 accepted steps; one persistent launch."""
+    seed 3; controlled RK45 at tol 1e-10, T_end = 100, cap 1e4 accepted steps.  Each lattice class runs on the
+    on-chip Dormand-Prince kernel with the tiling its autotuner picked (short runs before the timed call); the
+    classes' launches run concurrently on the owner handle's streams."""
     from classical_mcmc_spin_b200 import gpu_api
     from classical_mcmc_spin_b200.lattice import Lattice
     from classical_mcmc_spin_b200.states import random_unit_spins
@@ -207,6 +209,15 @@ def leg_uneven(torch, dev, max_steps=10000, T1=100.0, B=512):
         lat, h = handles[int(pick[b])]
         specs.append(dict(handle=h, state=random_unit_spins(lat.lattice_size, 3000 + b).ravel(), T0=0.0, T1=T1,
                           dt=0.01, max_rows=max_steps + 2))
+    # tiling of each lattice class (CTAs per trajectory x threads x sites per thread) by the autotuner
+    tilings = {}
+    t_tune = time.perf_counter()
+    for k, (lat, h) in handles.items():
+        gpu_api.set_tolerances(h, 1e-10, 1e-10)
+        gpu_api.set_gpu_spins(h, random_unit_spins(lat.lattice_size, 2999).ravel())
+        best, _ = h.autotune_rk45(int((pick == k).sum()), 40)     # the class's own batch size: its occupancy
+        tilings[f"{opts[k][0]}_L{opts[k][1]}"] = next(n for i, n, _ in h.rk45_variants() if i == best)
+    t_tune = time.perf_counter() - t_tune
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     out = gpu_api.run_uneven(specs, "rk45", 1e-10, 1e-10, max_steps=max_steps)
@@ -220,7 +231,8 @@ def leg_uneven(torch, dev, max_steps=10000, T1=100.0, B=512):
     return {"value": work / wall, "unit": "accepted spin·RK45-steps/s", "wall_s": wall, "trajectories": B,
             "accepted_steps": acc, "rejected_steps": rej, "spin_steps": work, "tol": 1e-10, "T_end": T1,
             "types": {f"{opts[k][0]}_L{opts[k][1]}": int((pick == k).sum()) for k in handles},
-            "timing": "wall clock around the public call (host buffers in and out)"}
+            "tilings": tilings, "autotune_s": t_tune,
+            "timing": "wall clock around the public call (host buffers in and out); tilings tuned before"}
 
 
 def _adjoint_leg(torch, dev, build, theta, theta_target, n_params, B, S, dt, seed, ckpt):

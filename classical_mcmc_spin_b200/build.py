@@ -22,7 +22,7 @@ BUILD = PKG / "_build"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-O3"]
-SOURCES = ["cmd_api.cu", "resident.cu", "stream.cu", "global.cu", "adjoint.cu", "noalloc.cu", "mixed_api.cu",
+SOURCES = ["cmd_api.cu", "resident.cu", "stream.cu", "global.cu", "rk45.cu", "adjoint.cu", "noalloc.cu", "mixed_api.cu",
            "spectrum.cu", "lattice_host.cpp"]
 DRIVER = PKG / "cmd_spin_solver"          # command-line driver (csrc/spin_solver.cpp) over the C ABI
 

@@ -13,6 +13,7 @@
 #include "rk4_cluster.cuh"
 #include "rk_global.cuh"
 
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 
@@ -398,6 +399,9 @@ int cmd_destroy(cmd_handle* h) {
                       &h->awork, &h->ackpt, &h->aseg, &h->amloc, &h->aout, &h->ameta, &h->ain,
                       &h->sbuf, &h->spart, &h->sgpart, &h->chunk_states, &h->chunk_rows, &h->cnbr2, &h->cnbr4, &h->cnbr8, &h->cnbr16, &h->cnbr_all})
         b->release();
+    for (cudaStream_t s2 : h->aux_streams) cudaStreamSynchronize(s2);
+    for (cudaEvent_t e2 : h->aux_events) cudaEventDestroy(e2);
+    for (cudaStream_t s2 : h->aux_streams) cudaStreamDestroy(s2);
     if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -1122,6 +1126,85 @@ int cmd_autotune(cmd_handle* h, int64_t B, int64_t n_steps, int32_t* best, doubl
     if (rc != CMD_OK) return rc;
     if (win < 0) return no_instance(h->lay);
     h->variant = win;
+    if (best) *best = win;
+    return CMD_OK;
+}
+
+int cmd_rk45_variant_count(void) { return rk45_variant_count(); }
+
+int cmd_rk45_variant_info(cmd_handle* h, int32_t idx, char* name, int32_t name_len, int32_t* fits) {
+    cmd::clear_error();
+    if (idx < 0 || idx >= rk45_variant_count()) return fail(CMD_ERR_INVALID_ARG, "tiling index out of range");
+    if (name && name_len > 0) {
+        std::strncpy(name, rk45_variant_name(idx), (size_t)name_len - 1);
+        name[name_len - 1] = 0;
+    }
+    if (fits) *fits = (h && rk45_fits(idx, h->lay)) ? 1 : 0;
+    return CMD_OK;
+}
+
+int cmd_set_rk45_variant(cmd_handle* h, int32_t idx) {
+    cmd::clear_error();
+    if (int rc = check_handle(h, false)) return rc;
+    if (idx < -2 || idx >= rk45_variant_count()) return fail(CMD_ERR_INVALID_ARG, "tiling index out of range");
+    if (idx >= 0 && !rk45_fits(idx, h->lay))
+        return fail(CMD_ERR_UNSUPPORTED, std::string(rk45_variant_name(idx)) + " does not hold this lattice");
+    h->rk45_variant = idx;
+    return CMD_OK;
+}
+
+int cmd_get_rk45_variant(cmd_handle* h, int32_t* idx) {
+    cmd::clear_error();
+    if (int rc = check_handle(h, false)) return rc;
+    if (!idx) return fail(CMD_ERR_INVALID_ARG, "NULL output");
+    const int v = rk45_pick(h);
+    *idx = v < 0 ? -2 : v;
+    return CMD_OK;
+}
+
+int cmd_autotune_rk45(cmd_handle* h, int64_t B, int64_t n_steps, int32_t* best, double* ms) {
+    cmd::clear_error();
+    if (int rc = check_handle(h, true)) return rc;
+    if (B <= 0 || B > (1 << 20) || n_steps <= 0) return fail(CMD_ERR_INVALID_ARG, "bad autotune size");
+    const int64_t max_rows = n_steps + 2, N3 = h->N * 3;
+    if (int rc = h->tune_obs.ensure((size_t)B * (max_rows * 11 + N3) * sizeof(double))) return rc;
+    double* rows = h->tune_obs.as<double>();
+    double* yout = rows + B * max_rows * 11;
+    std::vector<GJob> jobs(B);
+    for (int64_t b = 0; b < B; ++b) {
+        GJob& j = jobs[b];
+        j.h = h;
+        j.y0 = h->state.as<double>();
+        j.yout = yout + b * N3;
+        j.rows = rows + b * max_rows * 11;
+        j.max_rows = max_rows;
+        j.T0 = 0.0;
+        j.T1 = 1e300;
+        j.dt0 = 0.01;
+    }
+    const int saved = h->rk45_variant;
+    int win = -1;
+    double best_ms = 0.0;
+    int rc = CMD_OK;
+    for (int i = 0; i < rk45_variant_count() && rc == CMD_OK; ++i) {
+        if (ms) ms[i] = -1.0;
+        if (!rk45_fits(i, h->lay)) continue;
+        h->rk45_variant = i;
+        double t = 0.0;
+        std::vector<long long> stats;
+        for (int rep = 0; rep < 2 && rc == CMD_OK; ++rep) {     // first run warms up
+            const auto t0 = std::chrono::steady_clock::now();
+            rc = run_global(h, jobs, kModeRK45, h->abs_tol, h->rel_tol, n_steps, stats);
+            t = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        }
+        if (rc != CMD_OK) break;
+        if (ms) ms[i] = t;
+        if (win < 0 || t < best_ms) { win = i; best_ms = t; }
+    }
+    h->rk45_variant = saved;
+    if (rc != CMD_OK) return rc;
+    if (win < 0) return fail(CMD_ERR_UNSUPPORTED, "no on-chip RK45 tiling holds this lattice");
+    h->rk45_variant = win;
     if (best) *best = win;
     return CMD_OK;
 }

@@ -6,8 +6,10 @@
 //   resident.cu  resident RK4 (one CTA or a 2-/4-CTA cluster per trajectory),
 //                variant table, autotuner support
 //   stream.cu    streamed RK4 stages and the streamed adjoint
-//   global.cu    global-state integrator (fixed-step methods) and the on-chip
-//                controlled Dormand-Prince kernels
+//   global.cu    global-state integrator (fixed-step methods; controlled
+//                Dormand-Prince where no on-chip tiling holds the lattice) and
+//                the dispatch of controlled batches
+//   rk45.cu      on-chip controlled Dormand-Prince tilings and their launches
 //   adjoint.cu   resident and per-trajectory discrete adjoint, cmd_adjoint_rk4
 //   noalloc.cu   allocation-free batch entry point and its static scratch
 #pragma once
@@ -23,6 +25,7 @@
 #include "cmd.h"
 #include "cmd_internal.h"
 #include "rk4_resident.cuh"
+#include "rk_global.cuh"
 
 #define CUDA_TRY(expr)                                                                   \
     do {                                                                                 \
@@ -71,6 +74,8 @@ struct cmd_handle {
     cmd::DevBuf cnbr_all;       // RK45 on-chip kernels: every slot's partner word per site (built on first use)
     int cnbr_all_cs = 0;        // cluster size cnbr_all was built for
     cudaStream_t copy_stream = nullptr;  // cmd_run_batch: device-to-host copies of finished chunks
+    std::vector<cudaStream_t> aux_streams;   // concurrent launches of an uneven batch (created on first use)
+    std::vector<cudaEvent_t> aux_events;
     bool has_state = false;
     int device = -1;            // device current at cmd_create (owns the stream and buffers)
     double* noalloc_base = nullptr;   // device address of the allocation-free scratch on `device`
@@ -229,6 +234,17 @@ int run_stream_adjoint(cmd_handle* h, const StreamAdjJob& j, int n_params, const
 // global-state kernel.
 int run_global(cmd_handle* owner, std::vector<GJob>& jobs, int mode, double abs_tol, double rel_tol,
                int64_t max_steps, std::vector<long long>& stats);
+
+// ---- rk45.cu: on-chip controlled Dormand-Prince tilings
+int rk45_variant_count();
+const char* rk45_variant_name(int i);
+bool rk45_fits(int i, const Layout& L);
+// The tiling a handle's trajectories use: its tuned pick, else the first that
+// holds the lattice; -1 when none does (or the handle forces the global-state kernel).
+int rk45_pick(const cmd_handle* h);
+// Launches trajectories d_traj[0..B) (all on h's lattice) with tiling `variant` on `st`.
+int rk45_launch(cmd_handle* h, int variant, const GTraj* d_traj, int64_t B, double abs_tol, double rel_tol,
+                int64_t max_steps, cudaStream_t st);
 
 // ---- noalloc.cu
 int noalloc_lookup(double** out);

@@ -1,0 +1,159 @@
+// rk45.cu -- launches of the on-chip controlled Dormand-Prince kernels
+// (rk45_onchip.cuh): the tilings compiled into the library (CTAs per
+// trajectory x threads per CTA), the partner-word tables of each tiling, and
+// the choice between them (the handle's pick, made by cmd_autotune_rk45, or
+// the smallest cluster that holds the lattice).
+#include "cmd_core.h"
+#include "rk45_onchip.cuh"
+
+#include <cstdio>
+
+namespace cmd {
+namespace {
+
+using R45Fn = int (*)(const cmd_handle*, const R45Args&, int64_t, cudaStream_t);
+
+struct R45Variant {
+    int NAT, Z, LZ, APT, CS, MAXT;
+    R45Fn fn;
+    const char* name;
+};
+
+// Cells per CTA and the padded per-atom row of a tiling.
+void r45_shape(const R45Variant& v, int64_t G, int64_t* Gc, int64_t* Gp) {
+    *Gc = (G + v.CS - 1) / v.CS;
+    *Gp = (*Gc + 31) / 32 * 32;
+}
+
+template <int NAT, int Z, int LZ, int APT, int CS, int MAXT>
+int launch_r45(const cmd_handle* h, const R45Args& a, int64_t B, cudaStream_t st) {
+    auto kern = rk45_onchip_kernel<NAT, Z, LZ, APT, CS, MAXT>;
+    const int threads = NAT / APT * a.Gp;
+    const size_t smem = (size_t)r45_smem_doubles(NAT, a.Gp, CS, MAXT) * sizeof(double);
+    if (threads > MAXT || smem > kMaxSmem) return fail(CMD_ERR_UNSUPPORTED, "lattice does not fit this RK45 tiling");
+    // Function attributes belong to the current device's context: set on every launch.
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
+    if (CS > 8) CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    Couplings<NAT, Z> cp;
+    fill_couplings<NAT, Z>(h, h->fd.data(), h->fd.data() + 3 * h->NA, cp);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(B * CS));
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CS;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = CS > 1 ? 1 : 0;
+    CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, cp, a));
+    return CMD_OK;
+}
+
+#define CMD_R45(NAT, Z, LZ, APT, CS, MAXT) \
+    R45Variant{NAT, Z, LZ, APT, CS, MAXT, &launch_r45<NAT, Z, LZ, APT, CS, MAXT>, \
+               "rk45_onchip<" #NAT "," #Z "," #LZ "> apt=" #APT " cs=" #CS " maxt=" #MAXT}
+
+// Tilings: atoms per thread (a whole cell, or fewer for more threads per SM) x
+// CTAs per trajectory x thread bound (registers per thread = 64K / bound).
+// Ordered by preference when nothing was tuned: the first that holds a lattice
+// is its default.  The order follows the uneven batch's lattices measured on a
+// B200 (accepted spin-steps per second, tol 1e-10): honeycomb up to 16x16 on
+// one CTA with a site per thread, 24x24 and 32x32 on 2-CTA clusters with a
+// cell per thread; pyrochlore 4^3 / 6^3 / 8^3 conventional cells on 2-, 4- and
+// 8-CTA clusters with two sites per thread.
+const R45Variant kR45[] = {
+    // honeycomb (2-atom cells, 3 bonds per site)
+    CMD_R45(2, 3, 1, 1, 1, 512),
+    CMD_R45(2, 3, 1, 2, 2, 512),
+    CMD_R45(2, 3, 1, 2, 1, 256),
+    CMD_R45(2, 3, 1, 2, 4, 256),
+    CMD_R45(2, 3, 1, 2, 8, 256),
+    CMD_R45(2, 3, 1, 1, 2, 1024),
+    // pyrochlore (4-atom groups, 6 bonds per site)
+    CMD_R45(4, 6, 3, 2, 2, 256),
+    CMD_R45(4, 6, 3, 2, 4, 512),
+    CMD_R45(4, 6, 3, 2, 8, 512),
+    CMD_R45(4, 6, 3, 2, 1, 512),
+    CMD_R45(4, 6, 3, 2, 16, 256),
+    CMD_R45(4, 6, 3, 4, 1, 256),
+    CMD_R45(4, 6, 3, 4, 4, 256),
+    CMD_R45(4, 6, 3, 4, 8, 256),
+    CMD_R45(4, 6, 3, 1, 2, 512),
+};
+constexpr int kNumR45 = (int)(sizeof(kR45) / sizeof(kR45[0]));
+
+// Partner words [G][NA][Z-LZ] of a tiling (the bonds that leave the cell): slot
+// m of site (g, at) holds (rank << 24) | ((partner atom * 3) * Gp + partner cell
+// - rank * Gc), the partner's slot in its CTA's stage buffer.
+int upload_partner_words(cmd_handle* h, int cs, int64_t Gc, int64_t Gp) {
+    if (h->cnbr_all_cs == cs && h->cnbr_all.p) return CMD_OK;
+    const Layout& L = h->lay;
+    const int NA = L.NA, NL = L.Z - L.LZ;
+    const int64_t G = L.G;
+    std::vector<int> w(std::max<size_t>((size_t)G * NA * NL, 1), 0);
+    for (size_t i = 0; i < L.nbr.size(); ++i) {
+        const int64_t off = L.nbr[i];                 // (atom*3)*G + cell of the resident layout
+        const int64_t pat = off / (3 * G), gp = off - pat * 3 * G;
+        const int64_t r = gp / Gc, l = gp - r * Gc;
+        w[i] = (int)((r << kClusterRankShift) | (pat * 3 * Gp + l));
+    }
+    h->cnbr_all_cs = 0;
+    if (int rc = h->cnbr_all.ensure(w.size() * sizeof(int))) return rc;
+    CUDA_TRY(cudaMemcpy(h->cnbr_all.p, w.data(), w.size() * sizeof(int), cudaMemcpyHostToDevice));
+    h->cnbr_all_cs = cs;
+    return CMD_OK;
+}
+
+}  // namespace
+
+int rk45_variant_count() { return kNumR45; }
+const char* rk45_variant_name(int i) { return (i >= 0 && i < kNumR45) ? kR45[i].name : ""; }
+
+bool rk45_fits(int i, const Layout& L) {
+    if (i < 0 || i >= kNumR45) return false;
+    const R45Variant& v = kR45[i];
+    if (!L.uniform || v.NAT != L.NA || v.Z != L.Z || v.LZ != L.LZ) return false;
+    int64_t Gc, Gp;
+    r45_shape(v, L.G, &Gc, &Gp);
+    if (v.CS > 1 && Gc < 32) return false;                      // a cluster only for lattices one CTA cannot hold well
+    if (v.NAT / v.APT * Gp > v.MAXT) return false;
+    if ((size_t)r45_smem_doubles(v.NAT, (int)Gp, v.CS, v.MAXT) * sizeof(double) > kMaxSmem) return false;
+    if (6 * (int64_t)v.NAT * 3 * Gp >= (1 << kClusterRankShift)) return false;
+    return true;
+}
+
+int rk45_pick(const cmd_handle* h) {
+    if (h->rk45_variant == -2) return -1;                      // forced onto the global-state kernel
+    if (h->rk45_variant >= 0 && rk45_fits(h->rk45_variant, h->lay)) return h->rk45_variant;
+    for (int i = 0; i < kNumR45; ++i)
+        if (rk45_fits(i, h->lay)) return i;
+    return -1;
+}
+
+int rk45_launch(cmd_handle* h, int variant, const GTraj* d_traj, int64_t B, double abs_tol, double rel_tol,
+                int64_t max_steps, cudaStream_t st) {
+    if (!rk45_fits(variant, h->lay)) return fail(CMD_ERR_UNSUPPORTED, "RK45 tiling does not hold this lattice");
+    const R45Variant& v = kR45[variant];
+    int64_t Gc, Gp;
+    r45_shape(v, h->lay.G, &Gc, &Gp);
+    if (int rc = upload_partner_words(h, v.CS, Gc, Gp)) return rc;
+    R45Args a{};
+    a.traj = d_traj;
+    a.pw = h->cnbr_all.as<int>();
+    a.G = (int)h->lay.G;
+    a.Gc = (int)Gc;
+    a.Gp = (int)Gp;
+    a.abs_tol = abs_tol;
+    a.rel_tol = rel_tol;
+    a.max_steps = max_steps;
+    a.width = h->width;
+    a.freq = h->freq;
+    a.frames = h->dframes.as<double>();
+    a.afm = h->dafm.as<double>();
+    return v.fn(h, a, B, st);
+}
+
+}  // namespace cmd

@@ -112,6 +112,23 @@ __device__ __forceinline__ void bond_acc(double& h, double j0, double j1, double
     h = fma(j2, p2, h);
 }
 
+template <int V>
+struct AtomTag {
+    static constexpr int value = V;
+};
+
+// f(AtomTag<at>) with `at` (0 <= at < NAT) as a compile-time constant, so the
+// couplings of the atom stay constant-bank operands.
+template <int NAT, int AT = 0, class F>
+__device__ __forceinline__ void with_atom(int at, F&& f) {
+    if constexpr (AT < NAT) {
+        if (at == AT)
+            f(AtomTag<AT>{});
+        else
+            with_atom<NAT, AT + 1>(at, f);
+    }
+}
+
 // h -= d1*f1 + d2*f2 as two fused multiply-adds.
 __device__ __forceinline__ void drive_acc(double& h, double d1, double d2, double f1, double f2) {
     h = fma(-d1, f1, h);

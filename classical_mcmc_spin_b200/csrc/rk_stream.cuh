@@ -67,23 +67,6 @@ struct StreamArgs {
 template <int NAT>
 constexpr int stream_cells() { return kStreamTile / NAT; }
 
-template <int V>
-struct AtomTag {
-    static constexpr int value = V;
-};
-
-// f(AtomTag<at>) with `at` (0 <= at < NAT) as a compile-time constant, so the
-// couplings of the atom stay constant-bank operands.
-template <int NAT, int AT = 0, class F>
-__device__ __forceinline__ void with_atom(int at, F&& f) {
-    if constexpr (AT < NAT) {
-        if (at == AT)
-            f(AtomTag<AT>{});
-        else
-            with_atom<NAT, AT + 1>(at, f);
-    }
-}
-
 template <int NAT>
 __device__ __forceinline__ void stream_site(int& at, int& g) {
     constexpr int CPT = stream_cells<NAT>();

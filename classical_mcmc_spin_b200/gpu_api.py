@@ -83,6 +83,35 @@ class GPULatticeDataHandle:
         check(nat.lib().cmd_autotune(self.ptr, int(B), int(n_steps), C.byref(best), dptr(ms)), "cmd_autotune")
         return best.value, ms
 
+    def rk45_variants(self) -> list:
+        """[(index, name, holds this lattice)] of the on-chip controlled Dormand-Prince tilings."""
+        L = nat.lib()
+        out = []
+        for i in range(L.cmd_rk45_variant_count()):
+            buf = C.create_string_buffer(128)
+            fits = C.c_int32()
+            check(L.cmd_rk45_variant_info(self.ptr, i, buf, 128, C.byref(fits)), "cmd_rk45_variant_info")
+            out.append((i, buf.value.decode(), bool(fits.value)))
+        return out
+
+    def set_rk45_variant(self, idx: int) -> None:
+        """Pins an RK45 tiling (-1: default choice, -2: the global-memory kernel)."""
+        check(nat.lib().cmd_set_rk45_variant(self.ptr, int(idx)), "cmd_set_rk45_variant")
+
+    def get_rk45_variant(self) -> int:
+        v = C.c_int32()
+        check(nat.lib().cmd_get_rk45_variant(self.ptr, C.byref(v)), "cmd_get_rk45_variant")
+        return v.value
+
+    def autotune_rk45(self, B: int, n_steps: int) -> tuple:
+        """Times every RK45 tiling that holds the lattice; pins and returns (best index, ms per tiling)."""
+        n = nat.lib().cmd_rk45_variant_count()
+        ms = np.zeros(n)
+        best = C.c_int32()
+        check(nat.lib().cmd_autotune_rk45(self.ptr, int(B), int(n_steps), C.byref(best), dptr(ms)),
+              "cmd_autotune_rk45")
+        return best.value, ms
+
     def layout_info(self) -> dict:
         info = np.zeros(6, np.int64)
         check(nat.lib().cmd_layout_info(self.ptr, iptr(info)), "cmd_layout_info")

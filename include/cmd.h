@@ -332,6 +332,31 @@ int cmd_set_variant(cmd_handle* h, int32_t idx);
 int cmd_get_variant(cmd_handle* h, int32_t* idx);
 int cmd_autotune(cmd_handle* h, int64_t B, int64_t n_steps, int32_t* best, double* ms);
 
+/*
+ * Tilings of the on-chip controlled Dormand-Prince kernel (CMD_RK45 in
+ * cmd_integrate and cmd_run_uneven): CTAs per trajectory (one CTA or a
+ * thread-block cluster of 2..16) x threads per CTA.  No reference counterpart;
+ * the reference's controlled stepper is the CPU path's Boost.Odeint
+ * make_controlled<runge_kutta_dopri5> (lattice.h:4072-4078), which every
+ * tiling follows step for step.
+ *   cmd_rk45_variant_count  number of tilings in the library
+ *   cmd_rk45_variant_info   name of tiling idx and whether it holds h's lattice
+ *   cmd_set_rk45_variant    pin a tiling for h (-1: the default choice, the
+ *                           smallest cluster that holds the lattice; -2: the
+ *                           global-memory kernel, which holds any size)
+ *   cmd_get_rk45_variant    tiling h uses now (-2: global-memory kernel)
+ *   cmd_autotune_rk45       time every tiling that holds h's lattice on B
+ *                           trajectories from h's current spins for n_steps
+ *                           accepted steps at h's tolerances (cmd_set_tolerances),
+ *                           pin the fastest; ms[cmd_rk45_variant_count()] gets
+ *                           the times (-1 where a tiling does not fit), may be NULL
+ */
+int cmd_rk45_variant_count(void);
+int cmd_rk45_variant_info(cmd_handle* h, int32_t idx, char* name, int32_t name_len, int32_t* fits);
+int cmd_set_rk45_variant(cmd_handle* h, int32_t idx);
+int cmd_get_rk45_variant(cmd_handle* h, int32_t* idx);
+int cmd_autotune_rk45(cmd_handle* h, int64_t B, int64_t n_steps, int32_t* best, double* ms);
+
 /* Host-only version of the layout analysis cmd_create performs (no CUDA
  * call): fills info[0..5] like cmd_layout_info, info[6] = leading local slots
  * per atom; returns CMD_ERR_UNSUPPORTED with the reason when no resident

@@ -172,3 +172,78 @@ def test_uneven_batch_rk4_max_steps_and_errors(api, oracle):
     assert out[0][2][1] == 50 and len(out[0][0]) == 51
     with pytest.raises(CmdError):
         api.run_uneven([dict(handle=h, state=s0, T0=0.0, T1=1.0, dt=0.01, max_rows=5)], "rk4")
+
+
+def _rk45_case(oracle, kind, L):
+    from classical_mcmc_spin_b200.lattice import Lattice
+    if kind == "kitaev":
+        return Lattice.kitaev(L, L, 1), oracle.OracleLattice.kitaev(L, L, 1)
+    kw = dict(Jzz=1.0, Jpm=0.05, Jpmpm=0.02)
+    return (Lattice.pyrochlore_non_kramer(L, L, L, h=0.2, field_direction=R111, cubic=True, **kw),
+            oracle.OracleLattice.pyrochlore_nk(L, L, L, h=0.2, direction=R111, cubic=True, **kw))
+
+
+@pytest.mark.parametrize("kind,L,driven", [("kitaev", 8, False), ("kitaev", 8, True), ("kitaev", 32, False),
+                                           ("pyro", 4, True), ("pyro", 6, False), ("pyro", 8, False)])
+def test_rk45_every_tiling_matches_oracle_controller(api, oracle, kind, L, driven):
+    """Every on-chip tiling that holds the lattice (one CTA, 2- to 16-CTA clusters; 512 or 1024 threads) and
+    the global-memory kernel: identical accepted / rejected counts, rows <= 1e-7, final state <= 1e-9."""
+    lat, o = _rk45_case(oracle, kind, L)
+    s0 = _spins(lat.lattice_size, 400 + L)
+    h = lat.to_gpu()
+    api.set_tolerances(h, 1e-10, 1e-10)
+    T1 = 1.0
+    if driven:
+        fin = np.tile(R111, lat.N_atoms)
+        api.set_gpu_pulse(h, lat.rotate_pulse(fin, fin), 0.6, 0.15, 1.3, 0.3, 0.55)
+        o.set_pulse(fin, 0.3, fin, 0.55, 0.6, 0.15, 1.3)
+    orows, ofin, ostats = o.md_dopri5(s0, 0.0, T1, 0.01, 1e-10, 1e-10)
+    tilings = [(i, n) for i, n, fits in h.rk45_variants() if fits]
+    assert tilings, "no on-chip tiling holds the lattice"
+    for idx, name in tilings + [(-2, "global-memory kernel")]:
+        h.set_rk45_variant(idx)
+        assert h.get_rk45_variant() == idx
+        api.set_gpu_spins(h, s0)
+        _, obs, times = api.integrate_gpu(h, 0.0, T1, 0.01, 1, "rk45", with_states=False, max_rows=20000)
+        assert len(times) == len(orows), (name, len(times), len(orows), ostats)
+        assert times[-1] == T1, name
+        assert np.abs(times - orows[:, 0]).max() <= 1e-7, name
+        assert np.abs(obs[:, :9] - orows[:, 1:10]).max() <= 1e-7, name
+        assert np.abs(obs[:, 9] - orows[:, 10]).max() <= 1e-7, name
+        assert np.abs(api.get_gpu_spins(h) - ofin).max() <= 1e-9, name
+    h.close()
+
+
+def test_rk45_tiling_autotuner_pins_a_fitting_tiling(api, oracle):
+    lat, o = _rk45_case(oracle, "kitaev", 32)
+    s0 = _spins(lat.lattice_size, 77)
+    h = lat.to_gpu()
+    api.set_tolerances(h, 1e-10, 1e-10)
+    api.set_gpu_spins(h, s0)
+    best, ms = h.autotune_rk45(4, 20)
+    fits = {i for i, _, f in h.rk45_variants() if f}
+    assert best in fits and h.get_rk45_variant() == best
+    assert all((ms[i] > 0) == (i in fits) for i in range(len(ms)))
+    api.set_gpu_spins(h, s0)
+    _, obs, times = api.integrate_gpu(h, 0.0, 0.5, 0.01, 1, "rk45", with_states=False, max_rows=20000)
+    orows, ofin, _ = o.md_dopri5(s0, 0.0, 0.5, 0.01, 1e-10, 1e-10)
+    assert len(times) == len(orows) and np.abs(obs[:, :9] - orows[:, 1:10]).max() <= 1e-7
+    h.close()
+
+
+def test_rk45_saved_states_on_chip(api, oracle):
+    """States of every accepted step (the trajectory output of integrate_gpu) from the on-chip kernel."""
+    lat, o = _rk45_case(oracle, "kitaev", 6)
+    s0 = _spins(lat.lattice_size, 78)
+    h = lat.to_gpu()
+    api.set_tolerances(h, 1e-8, 1e-8)
+    api.set_gpu_spins(h, s0)
+    assert h.get_rk45_variant() >= 0
+    traj, obs, times = api.integrate_gpu(h, 0.0, 0.6, 0.01, 1, "rk45", with_states=True, max_rows=20000)
+    h.set_rk45_variant(-2)
+    api.set_gpu_spins(h, s0)
+    traj2, obs2, times2 = api.integrate_gpu(h, 0.0, 0.6, 0.01, 1, "rk45", with_states=True, max_rows=20000)
+    assert len(traj) == len(traj2) == len(times)
+    np.testing.assert_array_equal(traj[0][1], s0)
+    assert max(np.abs(a[1] - b[1]).max() for a, b in zip(traj, traj2)) <= 1e-10
+    h.close()
