@@ -136,6 +136,7 @@ struct Variant {
     bool YREG;
     int TPC;
     int CS;                       // CTAs per trajectory (thread-block cluster), 1 = one CTA
+    bool lean;                    // rk4_lean_kernel (compile-time strides; every atom carries Z bonds)
     LaunchFn fn;
     const char* name;
 };

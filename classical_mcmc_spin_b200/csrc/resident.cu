@@ -4,6 +4,7 @@
 // layouts.
 #include "cmd_core.h"
 #include "rk4_cluster.cuh"
+#include "rk4_lean.cuh"
 
 namespace cmd {
 namespace {
@@ -27,6 +28,24 @@ int launch_one(const cmd_handle* h, const cmd::ResidentArgs& args, const double*
     cmd::ResidentArgs a = args;
     a.B = B;
     kern<<<(unsigned)((B + TPC - 1) / TPC), threads, smem, st>>>(cp, a);
+    CUDA_TRY(cudaGetLastError());
+    return CMD_OK;
+}
+
+template <int NAT, int Z, int LZ, int MAXT, int MINB>
+int launch_lean(const cmd_handle* h, const cmd::ResidentArgs& args, const double* d1, const double* d2,
+                int64_t B, cudaStream_t st) {
+    auto kern = cmd::rk4_lean_kernel<NAT, Z, LZ, MAXT, MINB>;
+    const int64_t G = h->lay.G;
+    const int threads = (int)((G + 31) / 32 * 32);
+    if (threads > MAXT) return fail(CMD_ERR_UNSUPPORTED, "lattice too large for this kernel variant");
+    const size_t smem = (size_t)cmd::lean_smem_doubles(NAT, MAXT) * sizeof(double);
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
+    cmd::Couplings<NAT, Z> cp;
+    fill_couplings<NAT, Z>(h, d1, d2, cp);
+    cmd::ResidentArgs a = args;
+    a.B = B;
+    kern<<<(unsigned)B, threads, smem, st>>>(cp, a);
     CUDA_TRY(cudaGetLastError());
     return CMD_OK;
 }
@@ -68,15 +87,19 @@ int launch_cluster(const cmd_handle* h, const cmd::ResidentArgs& args, const dou
 }
 
 #define CMD_VARIANT(NAT, Z, LZ, CPT, MAXT, MINB, YREG, TPC) \
-    Variant{NAT, Z, LZ, CPT, MAXT, MINB, YREG, TPC, 1, &launch_one<NAT, Z, LZ, CPT, MAXT, MINB, YREG, TPC>, \
+    Variant{NAT, Z, LZ, CPT, MAXT, MINB, YREG, TPC, 1, false, &launch_one<NAT, Z, LZ, CPT, MAXT, MINB, YREG, TPC>, \
             "rk4_resident<" #NAT "," #Z "," #LZ "> cpt=" #CPT " maxt=" #MAXT " minb=" #MINB " yreg=" #YREG \
             " tpc=" #TPC}
+#define CMD_LEAN(NAT, Z, LZ, MAXT, MINB) \
+    Variant{NAT, Z, LZ, 1, MAXT, MINB, true, 1, 1, true, &launch_lean<NAT, Z, LZ, MAXT, MINB>, \
+            "rk4_lean<" #NAT "," #Z "," #LZ "> maxt=" #MAXT " minb=" #MINB}
 #define CMD_CLUSTER(NAT, Z, LZ, CS, MAXT) \
-    Variant{NAT, Z, LZ, 1, MAXT, 1, true, 1, CS, &launch_cluster<NAT, Z, LZ, CS, MAXT>, \
+    Variant{NAT, Z, LZ, 1, MAXT, 1, true, 1, CS, false, &launch_cluster<NAT, Z, LZ, CS, MAXT>, \
             "rk4_cluster<" #NAT "," #Z "," #LZ "> cs=" #CS " maxt=" #MAXT}
 
 const Variant kVariants[] = {
     // 2-atom cells with 3 bonds per site (Kitaev / Heisenberg honeycomb)
+    CMD_LEAN(2, 3, 1, 640, 1),
     CMD_VARIANT(2, 3, 1, 1, 640, 1, true, 1),
     CMD_VARIANT(2, 3, 1, 2, 320, 2, false, 1),
     CMD_VARIANT(2, 3, 1, 3, 192, 3, false, 1),
@@ -93,6 +116,7 @@ const Variant kVariants[] = {
     CMD_CLUSTER(2, 3, 1, 2, 640),
     CMD_CLUSTER(2, 3, 1, 4, 640),
     // 4-atom cells with 6 bonds per site (nearest-neighbour pyrochlore)
+    CMD_LEAN(4, 6, 3, 256, 1),
     CMD_VARIANT(4, 6, 3, 1, 512, 1, true, 1),
     CMD_VARIANT(4, 6, 3, 2, 256, 2, false, 1),
     CMD_VARIANT(4, 6, 3, 2, 512, 1, false, 1),
@@ -135,6 +159,12 @@ const int* cluster_table(const cmd_handle* h, int cs) {
 
 bool variant_fits(const Variant& v, const Layout& L) {
     if (!L.uniform || v.NAT != L.NA || v.Z != L.Z || v.LZ != L.LZ) return false;
+    if (v.lean) {
+        for (int a = 0; a < L.NA; ++a)
+            if (L.zc[a] != L.Z) return false;
+        return (L.G + 31) / 32 * 32 <= v.MAXT &&
+               (size_t)lean_smem_doubles(v.NAT, v.MAXT) * sizeof(double) <= kMaxSmem;
+    }
     if (v.CS > 1) {
         const int64_t Gc = cluster_cells(L.G, v.CS);
         return Gc >= 32 && (Gc + 31) / 32 * 32 <= v.MAXT && cluster_smem(v.NAT, L.G, v.CS) <= kMaxSmem &&
@@ -222,7 +252,9 @@ int run_resident(cmd_handle* h, const RunSpec& r, cudaStream_t st, int32_t* laun
         a.drive = h->drive.as<double>();
     }
     static const std::vector<double> zeros(3 * 64, 0.0);
-    if (int rc = V.fn(h, a, r.d1 ? r.d1 : zeros.data(), r.d2 ? r.d2 : zeros.data(), r.B, st)) return rc;
+    const double* d1 = r.d1 ? r.d1 : zeros.data();
+    const double* d2 = r.d2 ? r.d2 : zeros.data();
+    if (int rc = V.fn(h, a, d1, d2, r.B, st)) return rc;
     ++nl;
     if (r.obs) {
         const int64_t n = r.B * rows;
@@ -241,7 +273,10 @@ int run_resident(cmd_handle* h, const RunSpec& r, cudaStream_t st, int32_t* laun
 }
 
 void variant_shape(const Variant& V, const Layout& L, int64_t* threads, int64_t* smem) {
-    if (V.CS > 1) {
+    if (V.lean) {
+        *threads = (L.G + 31) / 32 * 32;
+        *smem = (int64_t)lean_smem_doubles(V.NAT, V.MAXT) * (int64_t)sizeof(double);
+    } else if (V.CS > 1) {
         *threads = (cluster_cells(L.G, V.CS) + 31) / 32 * 32;
         *smem = (int64_t)cluster_smem(L.NA, L.G, V.CS);
     } else {
