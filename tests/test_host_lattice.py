@@ -70,7 +70,8 @@ def test_layout_plan_honeycomb_configs(native):
     assert rc == nat.CMD_OK
     assert list(info[[0, 1, 2, 6]]) == [2, 576, 3, 1]        # 2 atoms/cell, 576 cells, 3 bonds, 1 in-cell
     assert info[3] == 576 and info[4] == 1
-    assert info[5] == 2 * 1152 * 3 * 8 + (32 * 16 + 12) * 8
+    # the lean variant: two stage buffers with the component stride of its 640-thread bound
+    assert info[5] == 2 * 2 * 3 * 640 * 8 + (32 * 16 + 12) * 8
     rc, info, _ = _plan(Lattice.kitaev(32, 32, 1))
     assert rc == nat.CMD_OK and info[4] == 2 and info[3] == 512
 
