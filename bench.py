@@ -384,6 +384,13 @@ def leg_pyrochlore(torch, dev, S=20000, S_adj=2000):
     clk.start()
     fwd = _forward_device(torch, dev, h, states, S, dt, streamed=True)
     fwd["clocks"] = clk.stop()
+    # the same run with every stage launched directly (no CUDA graph)
+    h.set_graphs(False)
+    direct = _forward_device(torch, dev, h, states, S, dt, streamed=True)
+    h.set_graphs(True)
+    fwd["direct_launches"] = {"value": direct["value"], "ms": direct["ms"], "launches": direct["launches"],
+                              "achieved_gbs": direct["achieved_gbs"]}
+    fwd["graph_over_direct"] = fwd["value"] / direct["value"]
     h.close()
     adj = _adjoint_leg(torch, dev, build, theta, np.array([1.0, 0.06, 0.03, 0.25]), 4, B, S_adj, dt, 5,
                        int(np.ceil(np.sqrt(S_adj))))

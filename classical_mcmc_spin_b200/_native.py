@@ -113,6 +113,7 @@ _SIGS = {
     "cmd_set_variant": (C.c_int, [C.c_void_p, C.c_int32]),
     "cmd_get_variant": (C.c_int, [C.c_void_p, _I32]),
     "cmd_autotune": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, _I32, _D]),
+    "cmd_set_graphs": (C.c_int, [C.c_void_p, C.c_int32]),
     "cmd_rk45_variant_count": (C.c_int, []),
     "cmd_rk45_variant_info": (C.c_int, [C.c_void_p, C.c_int32, C.c_char_p, C.c_int32, _I32]),
     "cmd_set_rk45_variant": (C.c_int, [C.c_void_p, C.c_int32]),

@@ -393,11 +393,12 @@ int cmd_create(const cmd_lattice_desc* d, cmd_handle** out) {
 int cmd_destroy(cmd_handle* h) {
     if (!h) return CMD_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    release_stream_graph(h);
     for (DevBuf* b : {&h->state, &h->nbr, &h->obs, &h->traj, &h->batch_states, &h->batch_out,
                       &h->pulses, &h->scratch, &h->dframes, &h->dafm, &h->times, &h->drive, &h->raw,
                       &h->tune_states, &h->tune_obs, &h->gwork, &h->gmeta, &h->gstat, &h->grows, &h->gqueue,
                       &h->awork, &h->ackpt, &h->aseg, &h->amloc, &h->aout, &h->ameta, &h->ain,
-                      &h->sbuf, &h->spart, &h->sgpart, &h->chunk_states, &h->chunk_rows, &h->cnbr2, &h->cnbr4, &h->cnbr8, &h->cnbr16, &h->cnbr_all})
+                      &h->sbuf, &h->spart, &h->sgpart, &h->snbase, &h->chunk_states, &h->chunk_rows, &h->cnbr2, &h->cnbr4, &h->cnbr8, &h->cnbr16, &h->cnbr_all})
         b->release();
     for (cudaStream_t s2 : h->aux_streams) cudaStreamSynchronize(s2);
     for (cudaEvent_t e2 : h->aux_events) cudaEventDestroy(e2);
@@ -1127,6 +1128,14 @@ int cmd_autotune(cmd_handle* h, int64_t B, int64_t n_steps, int32_t* best, doubl
     if (win < 0) return no_instance(h->lay);
     h->variant = win;
     if (best) *best = win;
+    return CMD_OK;
+}
+
+int cmd_set_graphs(cmd_handle* h, int32_t enable) {
+    cmd::clear_error();
+    if (int rc = check_handle(h, false)) return rc;
+    h->graphs = enable != 0;
+    if (!h->graphs) release_stream_graph(h);
     return CMD_OK;
 }
 

@@ -75,6 +75,12 @@ struct cmd_handle {
     int cnbr_all_cs = 0;        // cluster size cnbr_all was built for
     cudaStream_t copy_stream = nullptr;  // cmd_run_batch: device-to-host copies of finished chunks
     std::vector<cudaStream_t> aux_streams;   // concurrent launches of an uneven batch (created on first use)
+    // streamed RK4: the stage launches of one chunk of steps captured as a CUDA
+    // graph, replayed per chunk; rebuilt when any launch parameter changes
+    bool graphs = true;
+    cudaGraphExec_t stream_graph = nullptr;
+    std::vector<unsigned char> stream_graph_key;
+    cmd::DevBuf snbase;         // device step base of the replayed chunks
     std::vector<cudaEvent_t> aux_events;
     bool has_state = false;
     int device = -1;            // device current at cmd_create (owns the stream and buffers)
@@ -224,6 +230,8 @@ const int* cluster_table(const cmd_handle* h, int cs);
 void variant_shape(const Variant& V, const Layout& L, int64_t* threads, int64_t* smem);
 
 // ---- stream.cu
+// Drops the handle's captured launch sequence (after its stream is idle).
+void release_stream_graph(cmd_handle* h);
 int run_streamed(cmd_handle* h, const RunSpec& r, cudaStream_t st, int32_t* launches);
 int run_stream_adjoint(cmd_handle* h, const StreamAdjJob& j, int n_params, const std::vector<double>& DJ,
                        const std::vector<double>& DB, const std::vector<double>& DA, bool has_DA);

@@ -59,6 +59,9 @@ struct StreamArgs {
     // checkpoints [B][n_ckpt][V] every ckpt_every steps, or null
     double* ckpt;
     long long ckpt_every, n_ckpt, V;
+    // step base added to every stage launch's step argument, or null (base 0):
+    // a replayed launch sequence (CUDA graph) advances it on the device
+    const long long* nbase;
 };
 
 // Threads of a CTA: NAT groups of kStreamTile/NAT consecutive threads, group
@@ -232,8 +235,9 @@ __device__ __forceinline__ void stream_store_partial(const StreamArgs& a, int b,
 template <int NAT, int Z, int LZ>
 __global__ void __launch_bounds__(kStreamTile, 4)
 stream_stage_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_constant__ StreamArgs a, int s,
-                    long long n, SVec Yin, SVec y, SVec acc, SVec Ynext, int with_obs) {
+                    long long n_arg, SVec Yin, SVec y, SVec acc, SVec Ynext, int with_obs) {
     constexpr int NR = 3 * NAT + 1;
+    const long long n = (a.nbase ? *a.nbase : 0) + n_arg;
     __shared__ double red[32 * kRedStride];
     __shared__ double tot[16];
     const int b = blockIdx.y;
@@ -264,6 +268,11 @@ stream_stage_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_c
         });
     }
     if (s == 0 && with_obs) stream_store_partial<NR>(a, b, o, red);
+}
+
+// Advances the step base of a replayed launch sequence by k steps.
+static __global__ void stream_advance_kernel(long long* nbase, long long k) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *nbase += k;
 }
 
 // Observables' partials of y (the state after the last step).

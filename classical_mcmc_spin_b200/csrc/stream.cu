@@ -7,6 +7,56 @@
 namespace cmd {
 namespace {
 
+// Steps of the streamed RK4 loop: enqueue(k) launches the four stages of step
+// base + k, base read by the kernels from h->snbase.  With graphs on and at
+// least two chunks of work, one chunk of kChunk steps (4 kChunk stage launches
+// and a base advance) is captured once per distinct set of launch parameters
+// (`key`), kept in the handle and replayed; the remaining steps are launched
+// directly.  The kernels see the same step numbers either way.
+constexpr int64_t kChunk = 128;
+
+template <class F>
+int run_steps(cmd_handle* h, cudaStream_t st, int64_t S, const std::vector<unsigned char>& key, F&& enqueue,
+              int32_t* nl) {
+    CUDA_TRY(cudaMemsetAsync(h->snbase.p, 0, sizeof(long long), st));
+    int64_t done = 0;
+    if (h->graphs && S >= 2 * kChunk) {
+        if (!h->stream_graph || h->stream_graph_key != key) {
+            release_stream_graph(h);
+            cudaGraph_t g = nullptr;
+            CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            for (int64_t k = 0; k < kChunk; ++k) enqueue(k);
+            stream_advance_kernel<<<1, 32, 0, st>>>(h->snbase.as<long long>(), kChunk);
+            const cudaError_t e = cudaStreamEndCapture(st, &g);
+            if (e != cudaSuccess || !g) return fail(CMD_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
+            const cudaError_t e2 = cudaGraphInstantiate(&h->stream_graph, g, 0);
+            cudaGraphDestroy(g);
+            if (e2 != cudaSuccess) {
+                h->stream_graph = nullptr;
+                return fail(CMD_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e2));
+            }
+            h->stream_graph_key = key;
+        }
+        for (; done + kChunk <= S; done += kChunk) {
+            CUDA_TRY(cudaGraphLaunch(h->stream_graph, st));
+            *nl += 4 * (int32_t)kChunk + 1;
+        }
+    }
+    for (int64_t k = 0; done + k < S; ++k) {
+        enqueue(k);
+        *nl += 4;
+        if ((k & 1023) == 0) CUDA_TRY(cudaGetLastError());
+    }
+    CUDA_TRY(cudaGetLastError());
+    return CMD_OK;
+}
+
+template <class T>
+void key_add(std::vector<unsigned char>& k, const T& v) {
+    const unsigned char* p = reinterpret_cast<const unsigned char*>(&v);
+    k.insert(k.end(), p, p + sizeof(T));
+}
+
 // ---------------------------------------------------------------------------
 // Streamed RK4 (rk_stream.cuh): lattices no resident variant holds.  One launch
 // per stage over (cell tile, trajectory); same RunSpec contract and outputs as
@@ -83,16 +133,40 @@ int stream_forward(cmd_handle* h, const RunSpec& r, cudaStream_t st, int32_t* la
     CUDA_TRY(cudaGetLastError());
     ++nl;
     const int with_obs = r.obs ? 1 : 0;
-    for (int64_t n = 0; n < r.n_steps; ++n) {
-        if (r.traj && n % r.save == 0) save_traj(n / r.save);
-        cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 0, n, y, y, acc, Ya, with_obs);
-        cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 1, n, Ya, y, acc, Yb, with_obs);
-        cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 2, n, Yb, y, acc, Ya, with_obs);
-        cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 3, n, Ya, y, acc, y, with_obs);
-        nl += 4;
-        if ((n & 1023) == 0) CUDA_TRY(cudaGetLastError());
+    if (r.traj) {                                    // states saved between steps: direct launches
+        for (int64_t n = 0; n < r.n_steps; ++n) {
+            if (n % r.save == 0) save_traj(n / r.save);
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 0, n, y, y, acc, Ya, with_obs);
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 1, n, Ya, y, acc, Yb, with_obs);
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 2, n, Yb, y, acc, Ya, with_obs);
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 3, n, Ya, y, acc, y, with_obs);
+            nl += 4;
+            if ((n & 1023) == 0) CUDA_TRY(cudaGetLastError());
+        }
+        CUDA_TRY(cudaGetLastError());
+    } else {
+        if (int rc = h->snbase.ensure(sizeof(long long))) return rc;
+        a.nbase = h->snbase.as<long long>();
+        std::vector<unsigned char> key;
+        key_add(key, 1);                             // forward stages of this NAT/Z/LZ
+        key_add(key, NAT * 100 + Z * 10 + LZ);
+        key_add(key, cp);
+        key_add(key, a);
+        key_add(key, y);
+        key_add(key, acc);
+        key_add(key, Ya);
+        key_add(key, Yb);
+        key_add(key, with_obs);
+        key_add(key, grid);
+        auto enqueue = [&](int64_t k) {
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 0, k, y, y, acc, Ya, with_obs);
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 1, k, Ya, y, acc, Yb, with_obs);
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 2, k, Yb, y, acc, Ya, with_obs);
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 3, k, Ya, y, acc, y, with_obs);
+        };
+        if (int rc = run_steps(h, st, r.n_steps, key, enqueue, &nl)) return rc;
+        a.nbase = nullptr;                           // the final observation below uses absolute steps
     }
-    CUDA_TRY(cudaGetLastError());
     if (r.traj) save_traj(rows - 1);
     if (r.obs) {
         cmd::stream_obs_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, y);
@@ -254,6 +328,15 @@ int stream_adjoint(cmd_handle* h, const StreamAdjJob& j, const std::vector<doubl
 
 // Threads per CTA and shared memory per CTA of variant V on layout L.
 }  // namespace
+
+void release_stream_graph(cmd_handle* h) {
+    if (h->stream_graph) {
+        cudaStreamSynchronize(h->stream);
+        cudaGraphExecDestroy(h->stream_graph);
+    }
+    h->stream_graph = nullptr;
+    h->stream_graph_key.clear();
+}
 
 int run_streamed(cmd_handle* h, const RunSpec& r, cudaStream_t st, int32_t* launches) {
     switch (global_type(h->lay)) {

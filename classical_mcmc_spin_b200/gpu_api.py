@@ -83,6 +83,10 @@ class GPULatticeDataHandle:
         check(nat.lib().cmd_autotune(self.ptr, int(B), int(n_steps), C.byref(best), dptr(ms)), "cmd_autotune")
         return best.value, ms
 
+    def set_graphs(self, enable: bool) -> None:
+        """Streamed RK4: replay captured CUDA graphs of the stage launches (default) or launch directly."""
+        check(nat.lib().cmd_set_graphs(self.ptr, int(bool(enable))), "cmd_set_graphs")
+
     def rk45_variants(self) -> list:
         """[(index, name, holds this lattice)] of the on-chip controlled Dormand-Prince tilings."""
         L = nat.lib()

@@ -333,6 +333,17 @@ int cmd_get_variant(cmd_handle* h, int32_t* idx);
 int cmd_autotune(cmd_handle* h, int64_t B, int64_t n_steps, int32_t* best, double* ms);
 
 /*
+ * Launch sequences of the streamed RK4 path (lattices no resident kernel
+ * holds; one launch per RK stage): with graphs on (the default) the stage
+ * launches of a chunk of 128 steps are captured once as a CUDA graph, kept in
+ * the handle and replayed, so a 2x10^4-step run makes 157 graph launches
+ * instead of 8x10^4 kernel launches; the results are the same either way.  No
+ * reference counterpart (the reference launches and synchronises every stage,
+ * integrator.cuh:115-139).  enable = 0 launches every stage directly.
+ */
+int cmd_set_graphs(cmd_handle* h, int32_t enable);
+
+/*
  * Tilings of the on-chip controlled Dormand-Prince kernel (CMD_RK45 in
  * cmd_integrate and cmd_run_uneven): CTAs per trajectory (one CTA or a
  * thread-block cluster of 2..16) x threads per CTA.  No reference counterpart;

@@ -139,3 +139,32 @@ def test_streamed_adjoint_pyrochlore_matches_tlm(native, oracle, path):
     lt, gt = oracle.loss_grad_tlm(ob(theta), [ob(e) for e in np.eye(4)], states[0], 0.0, dt, S, targets[0])
     assert abs(loss[0] - lt) <= 1e-12 * max(1.0, abs(lt))
     np.testing.assert_allclose(grad[0], gt, rtol=1e-9, atol=1e-12)
+
+
+def test_streamed_graph_replay_matches_direct_launches_and_oracle(api, oracle):
+    """Kitaev 64x64 (streamed), 300 steps under a two-pulse drive: two replays of the captured 128-step
+    chunk plus 44 direct steps give the same bits as launching every stage directly, and the oracle's
+    trajectory; a second call with other pulses rebuilds the graph (different launch parameters)."""
+    from classical_mcmc_spin_b200.lattice import Lattice
+    lat = Lattice.kitaev(64, 64, 1)
+    o = oracle.OracleLattice.kitaev(64, 64, 1)
+    h = lat.to_gpu()
+    assert _streamed(h)
+    s0 = _spins(lat.lattice_size, 23)
+    fin = np.tile(R111, 2)
+    fd = lat.rotate_pulse(fin, fin)
+    nsteps = 300
+    for t2 in ([0.0, 0.6], [0.9, 1.3]):
+        kw = dict(T0=-0.5, t1=[0.0, 0.2], t2=t2, a1=[0.5, 0.5], a2=[0.0, 0.5], d1=fd[:6], d2=fd[6:], width=0.5,
+                  freq=0.0, shared_initial=True)
+        h.set_graphs(True)
+        og, fg = api.run_batch(h, s0, nsteps, 0.01, **kw)
+        h.set_graphs(False)
+        od, fdir = api.run_batch(h, s0, nsteps, 0.01, **kw)
+        np.testing.assert_array_equal(og, od)
+        np.testing.assert_array_equal(fg, fdir)
+        st, oobs = oracle_batch(o, np.tile(s0, (2, 1)), kw["t1"], t2, kw["a1"], kw["a2"], fin, nsteps)
+        assert np.abs(og[:, :, :9] - oobs[:, :, :9]).max() <= TOL_M
+        assert np.abs(og[:, :, 9] - oobs[:, :, 9]).max() <= TOL_M
+        assert np.abs(fg - st).max() <= TOL_S
+    h.close()
