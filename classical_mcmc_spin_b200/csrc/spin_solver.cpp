@@ -450,7 +450,8 @@ void run_md(const Config& c, Model& m) {
         if (c.md_save_spins) write_npy(dir / "trajectory_spins.npy", r.states, {r.n, m.N, 3});
         std::ofstream(dir / "metadata.json")
             << Json().str("simulation_mode", c.mode).str("system", c.system).num("lattice_size", (double)m.N)
-                   .num("spin_dim", 3).num("N_atoms", m.na).num("T_start", c.md_time_start).num("T_end", c.md_time_end)
+                   .num("spin_dim", 3).num("N_atoms", m.na).num("dim1", c.L[0]).num("dim2", c.L[1])
+                   .num("dim3", c.L[2]).num("T_start", c.md_time_start).num("T_end", c.md_time_end)
                    .num("T_step", c.md_timestep).num("save_interval", (double)c.md_save_interval)
                    .str("integration_method", c.md_integrator).num("rows", (double)r.n).done()
             << "\n";
@@ -613,7 +614,8 @@ void run_2dcs(const Config& c, Model& m) {
     write_npy(dir / "spectrum_local.npy", sp, {3, n_tau, n_t});
     std::ofstream(dir / "metadata.json")
         << Json().str("simulation_mode", c.mode).str("system", c.system).num("lattice_size", (double)m.N)
-               .num("spin_dim", 3).num("N_atoms", m.na).num("pulse_amp", c.pump_amplitude)
+               .num("spin_dim", 3).num("N_atoms", m.na).num("dim1", c.L[0]).num("dim2", c.L[1]).num("dim3", c.L[2])
+               .num("pulse_amp", c.pump_amplitude)
                .num("pulse_width", c.pump_width).num("pulse_freq", c.pump_frequency).num("T_start", c.md_time_start)
                .num("T_end", c.md_time_end).num("T_step", c.md_timestep).num("tau_start", c.tau_start)
                .num("tau_end", c.tau_end).num("tau_step", c.tau_step).num("tau_steps", (double)n_tau)

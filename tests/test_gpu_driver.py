@@ -70,6 +70,12 @@ output_dir = {out}
     assert np.abs(np.loadtxt(d / "initial_spins.txt").ravel() - s0).max() == 0.0
     meta = json.loads((d / "metadata.json").read_text())
     assert meta["rows"] == len(t) and meta["integration_method"] == "rk4"
+    # the reference's trajectory.h5 layout from this run (hdf5_export)
+    from classical_mcmc_spin_b200 import hdf5_export
+    plan = {e.path: e for e in hdf5_export.plan_trajectory(d)}
+    np.testing.assert_array_equal(plan["/trajectory/times"].data, t)
+    assert plan["/trajectory/spins"].data.shape == spins.shape
+    assert list(plan["/metadata/dimensions"].data) == [int(meta["dim1"]), int(meta["dim2"]), int(meta["dim3"])]
 
 
 def test_driver_pump_probe(driver, tmp_path, oracle):
@@ -154,6 +160,11 @@ output_dir = {out}
     meta = json.loads((d / "metadata.json").read_text())
     assert meta["tau_steps"] == 5 and meta["pulse_amp"] == 0.4
     assert meta["m1_synthesized"] == 0 and meta["max_dsdt_no_drive"] > 1e-3     # random state: M1 integrated
+    # the reference's pump_probe_spectroscopy.h5 layout from this run (hdf5_export)
+    from classical_mcmc_spin_b200 import hdf5_export
+    plan = {e.path: e for e in hdf5_export.plan_pump_probe(d)}
+    np.testing.assert_array_equal(plan["/tau_scan/tau_3/M01_local"].data, M["local"][2][3])
+    assert plan["/metadata"].attrs["tau_steps"] == 5 and plan["/metadata"].attrs["dim1"] == 4
 
 
 @pytest.mark.parametrize("integrator", ["rk5", "ssprk53", "rk78", "bs"])
