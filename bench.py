@@ -171,7 +171,7 @@ def fp64_peak_tflops(torch) -> float:
 
 def profile_traffic():
     """DRAM bytes per launch from the committed ncu summary, if present."""
-    p = ROOT / "profiles" / "rk4_resident_2dcs_kitaev1152.md"
+    p = ROOT / "profiles" / "rk4_lean_2dcs_kitaev1152.md"
     if not p.exists():
         return None
     for line in p.read_text().splitlines():
