@@ -298,6 +298,10 @@ def _forward_device(torch, dev, h, states, S, dt, streamed):
     desc.final_states = d_fin.data_ptr()
     launches = C.c_int32()
     stream = torch.cuda.current_stream(dev)
+    if stream.cuda_stream == 0:
+        # stream 0 makes the library use the handle's own stream, which these events would not see
+        stream = torch.cuda.Stream(device=dev)
+    torch.cuda.synchronize(dev)
 
     def run(n):
         desc.n_steps = n

@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -80,6 +81,10 @@ struct cmd_handle {
     bool graphs = true;
     cudaGraphExec_t stream_graph = nullptr;
     std::vector<unsigned char> stream_graph_key;
+    // batched resident run / uneven batch: each call's launches captured and
+    // replayed as one graph, the executable graph updated in place per call
+    cudaGraphExec_t call_graph[2] = {nullptr, nullptr};
+    std::vector<unsigned char> call_sig[2];   // kernels and launch shapes of call_graph[i]
     cmd::DevBuf snbase;         // device step base of the replayed chunks
     std::vector<cudaEvent_t> aux_events;
     bool has_state = false;
@@ -230,8 +235,18 @@ const int* cluster_table(const cmd_handle* h, int cs);
 void variant_shape(const Variant& V, const Layout& L, int64_t* threads, int64_t* smem);
 
 // ---- stream.cu
-// Drops the handle's captured launch sequence (after its stream is idle).
+// Drops the handle's captured launch sequences (after its stream is idle).
 void release_stream_graph(cmd_handle* h);
+// Graph slots of graph_call.
+constexpr int kGraphResident = 0, kGraphUneven = 1;
+// Runs enqueue() (stream-ordered work on st and on streams that join st; no
+// synchronous calls) through a CUDA graph when the handle's graphs are on and
+// st can be captured (not a default stream, not already capturing): the
+// launches are captured, the handle's executable graph of `slot` is updated
+// with them (instantiated when the launch topology changed) and launched on st.
+// Otherwise enqueue() runs directly.  Either way the same kernels run with the
+// same arguments.
+int graph_call(cmd_handle* h, int slot, cudaStream_t st, const std::function<int()>& enqueue);
 int run_streamed(cmd_handle* h, const RunSpec& r, cudaStream_t st, int32_t* launches);
 int run_stream_adjoint(cmd_handle* h, const StreamAdjJob& j, int n_params, const std::vector<double>& DJ,
                        const std::vector<double>& DB, const std::vector<double>& DA, bool has_DA);
@@ -251,6 +266,10 @@ bool rk45_fits(int i, const Layout& L);
 // The tiling a handle's trajectories use: its tuned pick, else the first that
 // holds the lattice; -1 when none does (or the handle forces the global-state kernel).
 int rk45_pick(const cmd_handle* h);
+// Uploads the partner words tiling `variant` reads (synchronous; a no-op when
+// they are current).  rk45_launch does it too; call it first where the launch
+// must not synchronise (inside a stream capture).
+int rk45_prepare(cmd_handle* h, int variant);
 // Launches trajectories d_traj[0..B) (all on h's lattice) with tiling `variant` on `st`.
 int rk45_launch(cmd_handle* h, int variant, const GTraj* d_traj, int64_t B, double abs_tol, double rel_tol,
                 int64_t max_steps, cudaStream_t st);

@@ -103,7 +103,6 @@ int run_global(cmd_handle* owner, std::vector<GJob>& jobs, int mode, double abs_
     CUDA_TRY(cudaMemsetAsync(owner->gqueue.p, 0, sizeof(int), st));
     CUDA_TRY(cudaMemsetAsync(owner->gstat.p, 0, B * 4 * sizeof(long long), st));
     const cmd::GTraj* dtr = owner->gmeta.as<cmd::GTraj>();
-    // fork: every on-chip group on an auxiliary stream, after the uploads above
     while (owner->aux_streams.size() < gh.size() + 1) {
         cudaStream_t s2 = nullptr;
         cudaEvent_t e2 = nullptr;
@@ -112,53 +111,69 @@ int run_global(cmd_handle* owner, std::vector<GJob>& jobs, int mode, double abs_
         CUDA_TRY(cudaEventCreateWithFlags(&e2, cudaEventDisableTiming));
         owner->aux_events.push_back(e2);
     }
-    if (!gh.empty()) CUDA_TRY(cudaEventRecord(owner->aux_events.back(), st));
-    int64_t off = (int64_t)gl.size();
-    for (size_t k = 0; k < gh.size(); ++k) {
-        cudaStream_t sk = owner->aux_streams[k];
-        CUDA_TRY(cudaStreamWaitEvent(sk, owner->aux_events.back(), 0));
-        const int64_t n = (int64_t)gj[k].size();
-        if (int rc = rk45_launch(gh[k], tiling[gj[k][0]], dtr + off, n, abs_tol, rel_tol, max_steps, sk)) return rc;
-        CUDA_TRY(cudaEventRecord(owner->aux_events[k], sk));
-        off += n;
-    }
-    if (!gl.empty()) {
-        cmd::GArgs a{};
-        a.traj = dtr;
-        a.B = (int)gl.size();
-        a.queue = owner->gqueue.as<int>();
-        a.mode = mode;
-        a.abs_tol = abs_tol;
-        a.rel_tol = rel_tol;
-        a.max_steps = max_steps;
-        const cmd_handle* any = src[0] ? src[0] : src[1];
-        a.width = any->width;
-        a.freq = any->freq;
-        cmd::Couplings<2, 3> c0;
-        cmd::Couplings<4, 6> c1;
-        std::memset(&c0, 0, sizeof(c0));
-        std::memset(&c1, 0, sizeof(c1));
-        if (src[0]) {
-            fill_couplings<2, 3>(src[0], src[0]->fd.data(), src[0]->fd.data() + 3 * src[0]->NA, c0);
-            a.frames0 = src[0]->dframes.as<double>();
-            a.afm0 = src[0]->dafm.as<double>();
+    for (size_t k = 0; k < gh.size(); ++k)
+        if (int rc = rk45_prepare(gh[k], tiling[gj[k][0]])) return rc;
+    // fork: every on-chip group on an auxiliary stream after the uploads above,
+    // the global-state kernel on the owner's stream, join; one graph
+    const int rc = graph_call(owner, kGraphUneven, st, [&]() -> int {
+        if (!gh.empty()) CUDA_TRY(cudaEventRecord(owner->aux_events.back(), st));
+        int64_t off = (int64_t)gl.size();
+        for (size_t k = 0; k < gh.size(); ++k) {
+            cudaStream_t sk = owner->aux_streams[k];
+            CUDA_TRY(cudaStreamWaitEvent(sk, owner->aux_events.back(), 0));
+            const int64_t n = (int64_t)gj[k].size();
+            int rc2 = rk45_launch(gh[k], tiling[gj[k][0]], dtr + off, n, abs_tol, rel_tol, max_steps, sk);
+            CUDA_TRY(cudaEventRecord(owner->aux_events[k], sk));      // joined below even after a failed launch
+            if (rc2) {
+                for (size_t q = 0; q <= k; ++q) cudaStreamWaitEvent(st, owner->aux_events[q], 0);
+                return rc2;
+            }
+            off += n;
         }
-        if (src[1]) {
-            fill_couplings<4, 6>(src[1], src[1]->fd.data(), src[1]->fd.data() + 3 * src[1]->NA, c1);
-            a.frames1 = src[1]->dframes.as<double>();
-            a.afm1 = src[1]->dafm.as<double>();
+        if (!gl.empty()) {
+            cmd::GArgs a{};
+            a.traj = dtr;
+            a.B = (int)gl.size();
+            a.queue = owner->gqueue.as<int>();
+            a.mode = mode;
+            a.abs_tol = abs_tol;
+            a.rel_tol = rel_tol;
+            a.max_steps = max_steps;
+            const cmd_handle* any = src[0] ? src[0] : src[1];
+            a.width = any->width;
+            a.freq = any->freq;
+            cmd::Couplings<2, 3> c0;
+            cmd::Couplings<4, 6> c1;
+            std::memset(&c0, 0, sizeof(c0));
+            std::memset(&c1, 0, sizeof(c1));
+            if (src[0]) {
+                fill_couplings<2, 3>(src[0], src[0]->fd.data(), src[0]->fd.data() + 3 * src[0]->NA, c0);
+                a.frames0 = src[0]->dframes.as<double>();
+                a.afm0 = src[0]->dafm.as<double>();
+            }
+            if (src[1]) {
+                fill_couplings<4, 6>(src[1], src[1]->fd.data(), src[1]->fd.data() + 3 * src[1]->NA, c1);
+                a.frames1 = src[1]->dframes.as<double>();
+                a.afm1 = src[1]->dafm.as<double>();
+            }
+            auto kern = mode >= cmd::kModeEuler ? cmd::rk_global_kernel<2, 3, 1, 4, 6, 3, true>
+                                                : cmd::rk_global_kernel<2, 3, 1, 4, 6, 3, false>;
+            int dev = 0, nsm = 148, per_sm = 1;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0);
+            const int grid = (int)std::min<int64_t>((int64_t)gl.size(), (int64_t)nsm * std::max(per_sm, 1));
+            kern<<<grid, 256, 0, st>>>(c0, c1, a);
+            const cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) {
+                for (size_t k = 0; k < gh.size(); ++k) cudaStreamWaitEvent(st, owner->aux_events[k], 0);
+                return fail(CMD_ERR_CUDA, std::string("rk_global_kernel: ") + cudaGetErrorString(e));
+            }
         }
-        auto kern = mode >= cmd::kModeEuler ? cmd::rk_global_kernel<2, 3, 1, 4, 6, 3, true>
-                                            : cmd::rk_global_kernel<2, 3, 1, 4, 6, 3, false>;
-        int dev = 0, nsm = 148, per_sm = 1;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0);
-        const int grid = (int)std::min<int64_t>((int64_t)gl.size(), (int64_t)nsm * std::max(per_sm, 1));
-        kern<<<grid, 256, 0, st>>>(c0, c1, a);
-        CUDA_TRY(cudaGetLastError());
-    }
-    for (size_t k = 0; k < gh.size(); ++k) CUDA_TRY(cudaStreamWaitEvent(st, owner->aux_events[k], 0));   // join
+        for (size_t k = 0; k < gh.size(); ++k) CUDA_TRY(cudaStreamWaitEvent(st, owner->aux_events[k], 0));   // join
+        return CMD_OK;
+    });
+    if (rc != CMD_OK) return rc;
     stats.assign((size_t)B * 4, 0);
     CUDA_TRY(cudaMemcpyAsync(stats.data(), owner->gstat.p, B * 4 * sizeof(long long), cudaMemcpyDeviceToHost, st));
     return sync(owner);

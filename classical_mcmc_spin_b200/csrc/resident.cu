@@ -243,31 +243,36 @@ int run_resident(cmd_handle* h, const RunSpec& r, cudaStream_t st, int32_t* laun
         if (int rc = h->times.ensure(grid.size() * sizeof(double))) return rc;
         if (int rc = h->drive.ensure((size_t)r.B * r.n_steps * 6 * sizeof(double))) return rc;
         CUDA_TRY(cudaMemcpyAsync(h->times.p, grid.data(), grid.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-        const int64_t total = r.B * r.n_steps * 6;
-        const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 32);
-        cmd::drive_table_kernel<<<blocks, 256, 0, st>>>(r.pulses, h->times.as<double>(), r.n_steps, r.dt, r.width,
-                                                       r.freq, r.B, h->drive.as<double>());
-        CUDA_TRY(cudaGetLastError());
-        ++nl;
         a.drive = h->drive.as<double>();
     }
+    if (r.obs && V.NAT != 2 && V.NAT != 4) return fail(CMD_ERR_UNSUPPORTED, "no row finisher for this cell size");
     static const std::vector<double> zeros(3 * 64, 0.0);
     const double* d1 = r.d1 ? r.d1 : zeros.data();
     const double* d2 = r.d2 ? r.d2 : zeros.data();
-    if (int rc = V.fn(h, a, d1, d2, r.B, st)) return rc;
-    ++nl;
-    if (r.obs) {
-        const int64_t n = r.B * rows;
-        const double* fr = r.frames ? r.frames : h->dframes.as<double>();
-        const double* af = r.afm ? r.afm : h->dafm.as<double>();
-        switch (V.NAT) {
-            case 2: launch_finish<2>(a.raw, a.raw_stride, n, fr, af, r.n_sites, r.obs, st); break;
-            case 4: launch_finish<4>(a.raw, a.raw_stride, n, fr, af, r.n_sites, r.obs, st); break;
-            default: return fail(CMD_ERR_UNSUPPORTED, "no row finisher for this cell size");
+    // drive table, the resident kernel and the row finisher: one graph
+    const int rc = graph_call(h, kGraphResident, st, [&]() -> int {
+        if (a.drive) {
+            const int64_t total = r.B * r.n_steps * 6;
+            const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 32);
+            cmd::drive_table_kernel<<<blocks, 256, 0, st>>>(r.pulses, h->times.as<double>(), r.n_steps, r.dt,
+                                                           r.width, r.freq, r.B, h->drive.as<double>());
+            CUDA_TRY(cudaGetLastError());
+            ++nl;
         }
-        CUDA_TRY(cudaGetLastError());
+        if (int rc2 = V.fn(h, a, d1, d2, r.B, st)) return rc2;
         ++nl;
-    }
+        if (r.obs) {
+            const int64_t n = r.B * rows;
+            const double* fr = r.frames ? r.frames : h->dframes.as<double>();
+            const double* af = r.afm ? r.afm : h->dafm.as<double>();
+            if (V.NAT == 2) launch_finish<2>(a.raw, a.raw_stride, n, fr, af, r.n_sites, r.obs, st);
+            else launch_finish<4>(a.raw, a.raw_stride, n, fr, af, r.n_sites, r.obs, st);
+            CUDA_TRY(cudaGetLastError());
+            ++nl;
+        }
+        return CMD_OK;
+    });
+    if (rc != CMD_OK) return rc;
     if (launches) *launches = nl;
     return CMD_OK;
 }

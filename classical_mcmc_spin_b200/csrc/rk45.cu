@@ -133,13 +133,20 @@ int rk45_pick(const cmd_handle* h) {
     return -1;
 }
 
-int rk45_launch(cmd_handle* h, int variant, const GTraj* d_traj, int64_t B, double abs_tol, double rel_tol,
-                int64_t max_steps, cudaStream_t st) {
+int rk45_prepare(cmd_handle* h, int variant) {
     if (!rk45_fits(variant, h->lay)) return fail(CMD_ERR_UNSUPPORTED, "RK45 tiling does not hold this lattice");
     const R45Variant& v = kR45[variant];
     int64_t Gc, Gp;
     r45_shape(v, h->lay.G, &Gc, &Gp);
-    if (int rc = upload_partner_words(h, v.CS, Gc, Gp)) return rc;
+    return upload_partner_words(h, v.CS, Gc, Gp);
+}
+
+int rk45_launch(cmd_handle* h, int variant, const GTraj* d_traj, int64_t B, double abs_tol, double rel_tol,
+                int64_t max_steps, cudaStream_t st) {
+    if (int rc = rk45_prepare(h, variant)) return rc;
+    const R45Variant& v = kR45[variant];
+    int64_t Gc, Gp;
+    r45_shape(v, h->lay.G, &Gc, &Gp);
     R45Args a{};
     a.traj = d_traj;
     a.pw = h->cnbr_all.as<int>();

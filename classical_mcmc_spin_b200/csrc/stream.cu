@@ -330,12 +330,99 @@ int stream_adjoint(cmd_handle* h, const StreamAdjJob& j, const std::vector<doubl
 }  // namespace
 
 void release_stream_graph(cmd_handle* h) {
-    if (h->stream_graph) {
-        cudaStreamSynchronize(h->stream);
-        cudaGraphExecDestroy(h->stream_graph);
-    }
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->stream_graph) cudaGraphExecDestroy(h->stream_graph);
     h->stream_graph = nullptr;
     h->stream_graph_key.clear();
+    for (int i = 0; i < 2; ++i) {
+        if (h->call_graph[i]) cudaGraphExecDestroy(h->call_graph[i]);
+        h->call_graph[i] = nullptr;
+        h->call_sig[i].clear();
+    }
+}
+
+namespace {
+
+// The node types in order and, per kernel node, its function, grid, block,
+// dynamic shared memory and cluster shape: what an in-place update of an
+// executable graph may not change.  False when a query fails.
+bool graph_signature(cudaGraph_t g, std::vector<unsigned char>& sig) {
+    size_t n = 0;
+    if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess) return false;
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (n && cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return false;
+    sig.clear();
+    key_add(sig, n);
+    for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) != cudaSuccess) return false;
+        key_add(sig, (int)t);
+        if (t != cudaGraphNodeTypeKernel) continue;
+        cudaKernelNodeParams p{};
+        if (cudaGraphKernelNodeGetParams(nd, &p) != cudaSuccess) return false;
+        key_add(sig, p.func);
+        key_add(sig, p.gridDim);
+        key_add(sig, p.blockDim);
+        key_add(sig, p.sharedMemBytes);
+        cudaLaunchAttributeValue v{};                  // zeros where the node has no cluster shape
+        if (cudaGraphKernelNodeGetAttribute(nd, cudaLaunchAttributeClusterDimension, &v) != cudaSuccess) {
+            (void)cudaGetLastError();
+            v = cudaLaunchAttributeValue{};
+        }
+        key_add(sig, v.clusterDim.x);
+        key_add(sig, v.clusterDim.y);
+        key_add(sig, v.clusterDim.z);
+    }
+    return true;
+}
+
+}  // namespace
+
+int graph_call(cmd_handle* h, int slot, cudaStream_t st, const std::function<int()>& enqueue) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    const bool capture = h->graphs && st != nullptr && st != cudaStreamLegacy && st != cudaStreamPerThread &&
+                         cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone;
+    if (!capture) return enqueue();
+    // relaxed: the launch helpers set kernel attributes, which is not stream work
+    CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+    const int rc = enqueue();
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (rc != CMD_OK || e != cudaSuccess || !g) {
+        if (g) cudaGraphDestroy(g);
+        (void)cudaGetLastError();
+        if (rc != CMD_OK) return rc;
+        return fail(CMD_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
+    }
+    // Same kernels and launch shapes as the kept graph: update its arguments in
+    // place; otherwise (or when the update is refused) build a new one.
+    std::vector<unsigned char> sig;
+    const bool have_sig = graph_signature(g, sig);
+    (void)cudaGetLastError();
+    cudaGraphExec_t& ex = h->call_graph[slot];
+    bool updated = false;
+    if (ex && have_sig && sig == h->call_sig[slot]) {
+        cudaGraphExecUpdateResultInfo info{};
+        updated = cudaGraphExecUpdate(ex, g, &info) == cudaSuccess;
+        (void)cudaGetLastError();
+    }
+    if (ex && !updated) {
+        cudaStreamSynchronize(st);                    // the old graph's last launch is done
+        cudaGraphExecDestroy(ex);
+        ex = nullptr;
+    }
+    h->call_sig[slot] = have_sig ? sig : std::vector<unsigned char>();
+    if (!ex) {
+        const cudaError_t e2 = cudaGraphInstantiate(&ex, g, 0);
+        if (e2 != cudaSuccess) {
+            ex = nullptr;
+            cudaGraphDestroy(g);
+            return fail(CMD_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e2));
+        }
+    }
+    cudaGraphDestroy(g);
+    CUDA_TRY(cudaGraphLaunch(ex, st));
+    return CMD_OK;
 }
 
 int run_streamed(cmd_handle* h, const RunSpec& r, cudaStream_t st, int32_t* launches) {

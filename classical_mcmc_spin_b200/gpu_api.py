@@ -84,7 +84,8 @@ class GPULatticeDataHandle:
         return best.value, ms
 
     def set_graphs(self, enable: bool) -> None:
-        """Streamed RK4: replay captured CUDA graphs of the stage launches (default) or launch directly."""
+        """CUDA graphs (default on): streamed RK4 replays captured chunks of stage launches; batched resident
+        runs and uneven batches run each call's launches as one captured graph.  Off: direct launches."""
         check(nat.lib().cmd_set_graphs(self.ptr, int(bool(enable))), "cmd_set_graphs")
 
     def rk45_variants(self) -> list:

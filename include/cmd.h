@@ -333,13 +333,18 @@ int cmd_get_variant(cmd_handle* h, int32_t* idx);
 int cmd_autotune(cmd_handle* h, int64_t B, int64_t n_steps, int32_t* best, double* ms);
 
 /*
- * Launch sequences of the streamed RK4 path (lattices no resident kernel
- * holds; one launch per RK stage): with graphs on (the default) the stage
- * launches of a chunk of 128 steps are captured once as a CUDA graph, kept in
- * the handle and replayed, so a 2x10^4-step run makes 157 graph launches
- * instead of 8x10^4 kernel launches; the results are the same either way.  No
+ * CUDA graphs, on by default.  Streamed RK4 (lattices no resident kernel
+ * holds; one launch per RK stage): the stage launches of a chunk of 128 steps
+ * are captured once as a CUDA graph, kept in the handle and replayed, so a
+ * 2x10^4-step run makes 157 graph launches instead of 8x10^4 kernel launches.
+ * Batched resident runs (drive table, resident kernel, row finisher) and
+ * uneven batches (the per-lattice launches on the handle's auxiliary streams,
+ * forked from and joined to the call's stream): each call is captured and
+ * launched as one graph, the handle's executable graph updated in place when
+ * only arguments change.  Calls on a default stream, or on a stream the caller
+ * is capturing, launch directly.  The results are the same either way.  No
  * reference counterpart (the reference launches and synchronises every stage,
- * integrator.cuh:115-139).  enable = 0 launches every stage directly.
+ * integrator.cuh:115-139).  enable = 0 launches everything directly.
  */
 int cmd_set_graphs(cmd_handle* h, int32_t enable);
 
