@@ -15,6 +15,7 @@ using R45Fn = int (*)(const cmd_handle*, const R45Args&, int64_t, cudaStream_t);
 
 struct R45Variant {
     int NAT, Z, LZ, APT, CS, MAXT;
+    bool YK;                  // y and K1 in shared memory instead of registers
     R45Fn fn;
     const char* name;
 };
@@ -25,11 +26,11 @@ void r45_shape(const R45Variant& v, int64_t G, int64_t* Gc, int64_t* Gp) {
     *Gp = (*Gc + 31) / 32 * 32;
 }
 
-template <int NAT, int Z, int LZ, int APT, int CS, int MAXT>
+template <int NAT, int Z, int LZ, int APT, int CS, int MAXT, bool YK>
 int launch_r45(const cmd_handle* h, const R45Args& a, int64_t B, cudaStream_t st) {
-    auto kern = rk45_onchip_kernel<NAT, Z, LZ, APT, CS, MAXT>;
+    auto kern = rk45_onchip_kernel<NAT, Z, LZ, APT, CS, MAXT, YK>;
     const int threads = NAT / APT * a.Gp;
-    const size_t smem = (size_t)r45_smem_doubles(NAT, a.Gp, CS, MAXT) * sizeof(double);
+    const size_t smem = (size_t)r45_smem_doubles(NAT, a.Gp, CS, MAXT, YK) * sizeof(double);
     if (threads > MAXT || smem > kMaxSmem) return fail(CMD_ERR_UNSUPPORTED, "lattice does not fit this RK45 tiling");
     // Function attributes belong to the current device's context: set on every launch.
     CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxSmem));
@@ -53,20 +54,27 @@ int launch_r45(const cmd_handle* h, const R45Args& a, int64_t B, cudaStream_t st
 }
 
 #define CMD_R45(NAT, Z, LZ, APT, CS, MAXT) \
-    R45Variant{NAT, Z, LZ, APT, CS, MAXT, &launch_r45<NAT, Z, LZ, APT, CS, MAXT>, \
+    R45Variant{NAT, Z, LZ, APT, CS, MAXT, false, &launch_r45<NAT, Z, LZ, APT, CS, MAXT, false>, \
                "rk45_onchip<" #NAT "," #Z "," #LZ "> apt=" #APT " cs=" #CS " maxt=" #MAXT}
+#define CMD_R45_YK(NAT, Z, LZ, APT, CS, MAXT) \
+    R45Variant{NAT, Z, LZ, APT, CS, MAXT, true, &launch_r45<NAT, Z, LZ, APT, CS, MAXT, true>, \
+               "rk45_onchip<" #NAT "," #Z "," #LZ "> apt=" #APT " cs=" #CS " maxt=" #MAXT " yk"}
 
 // Tilings: atoms per thread (a whole cell, or fewer for more threads per SM) x
-// CTAs per trajectory x thread bound (registers per thread = 64K / bound).
-// Ordered by preference when nothing was tuned: the first that holds a lattice
-// is its default.  The order follows the uneven batch's lattices measured on a
-// B200 (accepted spin-steps per second, tol 1e-10): honeycomb up to 16x16 on
-// one CTA with a site per thread, 24x24 and 32x32 on 2-CTA clusters with a
-// cell per thread; pyrochlore 4^3 / 6^3 / 8^3 conventional cells on 2-, 4- and
-// 8-CTA clusters with two sites per thread.
+// CTAs per trajectory x thread bound (registers per thread = 64K / bound), and
+// where y and K1 live ("yk": the thread's own shared-memory slots, which frees
+// registers for the stages).  Ordered by preference when nothing was tuned: the
+// first that holds a lattice is its default.  The order follows the uneven
+// batch's lattices measured on a B200 (accepted spin-steps per second, tol
+// 1e-10): honeycomb up to 16x16 on one CTA with a site per thread, 24x24 and
+// 32x32 on 2-CTA clusters with a cell per thread (y, K1 in shared memory);
+// pyrochlore 4^3 / 6^3 conventional cells on 2- and 4-CTA clusters with two
+// sites per thread, 8^3 on 8-CTA clusters with a whole 4-site group per thread
+// (y, K1 in shared memory).
 const R45Variant kR45[] = {
     // honeycomb (2-atom cells, 3 bonds per site)
     CMD_R45(2, 3, 1, 1, 1, 512),
+    CMD_R45_YK(2, 3, 1, 2, 2, 512),
     CMD_R45(2, 3, 1, 2, 2, 512),
     CMD_R45(2, 3, 1, 2, 1, 256),
     CMD_R45(2, 3, 1, 2, 4, 256),
@@ -75,6 +83,7 @@ const R45Variant kR45[] = {
     // pyrochlore (4-atom groups, 6 bonds per site)
     CMD_R45(4, 6, 3, 2, 2, 256),
     CMD_R45(4, 6, 3, 2, 4, 512),
+    CMD_R45_YK(4, 6, 3, 4, 8, 256),
     CMD_R45(4, 6, 3, 2, 8, 512),
     CMD_R45(4, 6, 3, 2, 1, 512),
     CMD_R45(4, 6, 3, 2, 16, 256),
@@ -82,6 +91,8 @@ const R45Variant kR45[] = {
     CMD_R45(4, 6, 3, 4, 4, 256),
     CMD_R45(4, 6, 3, 4, 8, 256),
     CMD_R45(4, 6, 3, 1, 2, 512),
+    CMD_R45_YK(4, 6, 3, 2, 4, 512),
+    CMD_R45_YK(4, 6, 3, 4, 4, 256),
 };
 constexpr int kNumR45 = (int)(sizeof(kR45) / sizeof(kR45[0]));
 
@@ -120,7 +131,7 @@ bool rk45_fits(int i, const Layout& L) {
     r45_shape(v, L.G, &Gc, &Gp);
     if (v.CS > 1 && Gc < 32) return false;                      // a cluster only for lattices one CTA cannot hold well
     if (v.NAT / v.APT * Gp > v.MAXT) return false;
-    if ((size_t)r45_smem_doubles(v.NAT, (int)Gp, v.CS, v.MAXT) * sizeof(double) > kMaxSmem) return false;
+    if ((size_t)r45_smem_doubles(v.NAT, (int)Gp, v.CS, v.MAXT, v.YK) * sizeof(double) > kMaxSmem) return false;
     if (6 * (int64_t)v.NAT * 3 * Gp >= (1 << kClusterRankShift)) return false;
     return true;
 }

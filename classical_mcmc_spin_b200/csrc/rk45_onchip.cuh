@@ -68,11 +68,11 @@ struct R45Args {
 // Reduction values per warp: the observable partials padded to a power of two.
 __host__ __device__ constexpr int r45_nv(int nat) { return 3 * nat + 1 <= 8 ? 8 : 16; }
 
-// Shared memory of one CTA in doubles: two stage buffers, K2..K5, the per-warp
-// error maxima of every CTA [cs][maxt/32], rank 0's per-warp observable
-// partials [cs][maxt/32][nv] and the drive factors [12].
-__host__ __device__ constexpr long long r45_smem_doubles(int nat, int gp, int cs, int maxt) {
-    return 6LL * nat * 3 * gp + (long long)cs * (maxt / 32) * (1 + r45_nv(nat)) + 12;
+// Shared memory of one CTA in doubles: two stage buffers, K2..K5 (and, with
+// yk, y and K1), the per-warp error maxima of every CTA [cs][maxt/32], rank 0's
+// per-warp observable partials [cs][maxt/32][nv] and the drive factors [12].
+__host__ __device__ constexpr long long r45_smem_doubles(int nat, int gp, int cs, int maxt, bool yk = false) {
+    return (yk ? 8LL : 6LL) * nat * 3 * gp + (long long)cs * (maxt / 32) * (1 + r45_nv(nat)) + 12;
 }
 
 __device__ __forceinline__ uint32_t r45_map(uint32_t local, int rank) {
@@ -221,7 +221,7 @@ __device__ __forceinline__ void r45_rhs(int ag, const Couplings<NAT, Z>& cp, con
 // Observable partials of a thread: S of its APT atoms, then S.(H - B), padded.
 __host__ __device__ constexpr int r45_nvl(int apt) { return 3 * apt + 1 <= 4 ? 4 : (3 * apt + 1 <= 8 ? 8 : 16); }
 
-template <int NAT, int Z, int LZ, int APT, int CS, int MAXT>
+template <int NAT, int Z, int LZ, int APT, int CS, int MAXT, bool YK = false>
 __global__ void __launch_bounds__(MAXT, 1)
 rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_constant__ R45Args a) {
     constexpr int NL = Z - LZ;                       // bonds per atom leaving the cell
@@ -243,7 +243,7 @@ rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_co
     const GTraj& T = a.traj[blockIdx.x / CS];
     const int Gp = a.Gp, SB = NAT * 3 * Gp;
     double* Ks = smem + 2 * SB;                      // K2, K3, K4, K5: [4][SB], own slots
-    double* emx = smem + 6 * SB;                     // [CS][NWM] per-warp error maxima of every CTA
+    double* emx = smem + (YK ? 8 : 6) * SB;          // [CS][NWM] per-warp error maxima of every CTA
     double* obs = emx + CS * NWM;                    // [CS][NWM][NV] per-warp observable partials (rank 0 reads)
     double* drv = obs + CS * NWM * NV;               // [12] drive factors of stages 2..6 (pulse 1, 2)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
@@ -272,14 +272,24 @@ rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_co
     const uint32_t emx_slot = (uint32_t)__cvta_generic_to_shared(emx + rank * NWM + warp);
     const uint32_t obs_slot = (uint32_t)__cvta_generic_to_shared(obs + (rank * NWM + warp) * NV);
 
-    double y[APT][3], K1[APT][3], cur[APT][3];
+    // y and K1 of the thread's atoms: registers, or (YK) its own slots of two
+    // more shared-memory vectors, which leaves registers to the stages
+    double yr[APT][3], k1r[APT][3], cur[APT][3];
+    auto yref = [&](int i, int c) __attribute__((always_inline)) -> double& {
+        if constexpr (YK) return smem[6 * SB + me + (i * 3 + c) * Gp];
+        else return yr[i][c];
+    };
+    auto k1ref = [&](int i, int c) __attribute__((always_inline)) -> double& {
+        if constexpr (YK) return smem[7 * SB + me + (i * 3 + c) * Gp];
+        else return k1r[i][c];
+    };
 #pragma unroll
     for (int i = 0; i < APT; ++i)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            y[i][c] = own ? T.y0[((long long)g * NAT + ag * APT + i) * 3 + c] : 0.0;
-            cur[i][c] = y[i][c];
-            smem[me + (i * 3 + c) * Gp] = y[i][c];
+            yref(i, c) = own ? T.y0[((long long)g * NAT + ag * APT + i) * 3 + c] : 0.0;
+            cur[i][c] = yref(i, c);
+            smem[me + (i * 3 + c) * Gp] = yref(i, c);
         }
 
     auto rhs = [&](int in, uint32_t tok, double f1, double f2, double (&k)[APT][3]) __attribute__((always_inline)) {
@@ -346,7 +356,7 @@ rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_co
 #pragma unroll
                 for (int i = 0; i < APT; ++i)
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) dst[i * 3 + c] = y[i][c];
+                    for (int c = 0; c < 3; ++c) dst[i * 3 + c] = yref(i, c);
             }
             if (rank == 0 && warp == 0) {
                 double m[NR];
@@ -397,7 +407,7 @@ rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_co
 #pragma unroll
         for (int i = 0; i < APT; ++i)
 #pragma unroll
-            for (int c = 0; c < 3; ++c) K1[i][c] = k[i][c];
+            for (int c = 0; c < 3; ++c) k1ref(i, c) = k[i][c];
         if (!own)
 #pragma unroll
             for (int q = 0; q < NVL; ++q) part[q] = 0.0;
@@ -424,7 +434,7 @@ rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_co
 #pragma unroll
             for (int i = 0; i < APT; ++i)
 #pragma unroll
-                for (int c = 0; c < 3; ++c) publish(in, i, c, y[i][c] + dt * kR45A[0][0] * K1[i][c]);
+                for (int c = 0; c < 3; ++c) publish(in, i, c, yref(i, c) + dt * kR45A[0][0] * k1ref(i, c));
             tok = r45_sync<CS>();
             // stages 2..5: K_{r+2}, then the input of stage r+3 (y + dt a_{r+3,1} K1 + ...
             // + dt a_{r+3,r+2} K_{r+2}, added left to right); K2..K5 in own slots [r]
@@ -438,7 +448,7 @@ rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_co
                     for (int c = 0; c < 3; ++c) {
                         const int s = me + (i * 3 + c) * Gp;
                         Ks[r * SB + s] = k[i][c];
-                        double v = y[i][c] + dt * kR45A[r + 1][0] * K1[i][c];
+                        double v = yref(i, c) + dt * kR45A[r + 1][0] * k1ref(i, c);
                         for (int j = 0; j < r; ++j) v = v + dt * kR45A[r + 1][j + 1] * Ks[j * SB + s];
                         publish(in, i, c, v + dt * kR45A[r + 1][r + 1] * k[i][c]);
                     }
@@ -454,9 +464,9 @@ rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_co
                     const int s = me + (i * 3 + c) * Gp;
                     const double K3 = Ks[SB + s], K4 = Ks[2 * SB + s], K5 = Ks[3 * SB + s];
                     // the partial error goes to K2's slot (K2 is not read after stage 5)
-                    Ks[s] = dt * dc1 * K1[i][c] + dt * dc3 * K3 + dt * dc4 * K4 + dt * dc5 * K5 + dt * dc6 * k[i][c];
+                    Ks[s] = dt * dc1 * k1ref(i, c) + dt * dc3 * K3 + dt * dc4 * K4 + dt * dc5 * K5 + dt * dc6 * k[i][c];
                     publish(in, i, c,
-                            y[i][c] + dt * b1 * K1[i][c] + dt * b3 * K3 + dt * b4 * K4 + dt * b5 * K5 +
+                            yref(i, c) + dt * b1 * k1ref(i, c) + dt * b3 * K3 + dt * b4 * K4 + dt * b5 * K5 +
                                 dt * b6 * k[i][c]);
                 }
             tok = r45_sync<CS>();
@@ -472,7 +482,7 @@ rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_co
                 for (int c = 0; c < 3; ++c) {
                     const double ec = Ks[me + (i * 3 + c) * Gp] + dt * dc7 * k[i][c];
                     const double r =
-                        fabs(ec) / (a.abs_tol + a.rel_tol * (1.0 * fabs(y[i][c]) + 1.0 * dt * fabs(K1[i][c])));
+                        fabs(ec) / (a.abs_tol + a.rel_tol * (1.0 * fabs(yref(i, c)) + 1.0 * dt * fabs(k1ref(i, c))));
                     emax = fmax(emax, r);
                 }
             if (!own) {
@@ -496,8 +506,8 @@ rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_co
             for (int i = 0; i < APT; ++i)
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
-                    y[i][c] = cur[i][c];                 // the new solution, published in stage 6
-                    K1[i][c] = k[i][c];
+                    yref(i, c) = cur[i][c];                 // the new solution, published in stage 6
+                    k1ref(i, c) = k[i][c];
                 }
             record(t, obs_q);
             if (err < 0.5) {
@@ -514,7 +524,7 @@ rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_co
 #pragma unroll
         for (int i = 0; i < APT; ++i)
 #pragma unroll
-            for (int c = 0; c < 3; ++c) T.yout[((long long)g * NAT + ag * APT + i) * 3 + c] = y[i][c];
+            for (int c = 0; c < 3; ++c) T.yout[((long long)g * NAT + ag * APT + i) * 3 + c] = yref(i, c);
     if (rank == 0 && tid == 0 && T.stat) {
         T.stat[0] = nrow;
         T.stat[1] = acc_steps;

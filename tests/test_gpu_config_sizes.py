@@ -161,3 +161,40 @@ def test_config4_adjoint_48x48_checkpoint141_matches_tlm_and_fd(oracle):
         np.testing.assert_allclose(grad[:, q], fd, rtol=1e-6, atol=1e-6 * np.abs(grad).max())
     h.close()
     ht.close()
+
+
+def test_config5_adjoint_pyrochlore65536_matches_tlm_and_fd(oracle):
+    """The large-lattice adjoint at its own size: pyrochlore 16^3 conventional cells (65536 spins, streamed
+    kernels), parameters (Jzz, J+-, J+-+-, h along [111]) as in the benchmark's leg, 24 steps of dt = 0.005 with a
+    checkpoint every 5 steps (four full segments and a partial one): loss <= 1e-12, gradient <= 1e-9 against the
+    tangent-linear oracle and <= 1e-6 against central finite differences of the GPU forward."""
+    from classical_mcmc_spin_b200 import adjoint as A
+    from classical_mcmc_spin_b200.states import random_unit_spins
+    theta = np.array([1.0, 0.05, 0.02, 0.2])
+    build = lambda th: A.pyrochlore_lattice(th, 16, 16, 16, cubic=True)
+    lat = build(theta)
+    N, S, dt = lat.lattice_size, 24, 0.005
+    assert N == 65536
+    h, ht = lat.to_gpu(), build(np.array([1.0, 0.06, 0.03, 0.25])).to_gpu()
+    states = random_unit_spins(N, 5000).ravel()[None, :]
+    _, _, target = A.adjoint_rk4(ht, [], states, 0.0, dt, S, np.zeros((1, S + 1, 3)), forward_only=True)
+    loss, grad, _ = A.adjoint_rk4(h, A.basis_lattices(build, 4), states, 0.0, dt, S, target, checkpoint_every=5)
+    ob = lambda th: oracle.OracleLattice.pyrochlore_nk(16, 16, 16, h=th[3], direction=R111, cubic=True, Jzz=th[0],
+                                                       Jpm=th[1], Jpmpm=th[2])
+    lt, gt = oracle.loss_grad_tlm(ob(theta), [ob(e) for e in np.eye(4)], states[0], 0.0, dt, S, target[0])
+    assert abs(loss[0] - lt) <= 1e-12 * max(1.0, abs(lt))
+    np.testing.assert_allclose(grad[0], gt, rtol=1e-9, atol=1e-12 * np.abs(gt).max())
+    eps = 1e-5
+    for q in range(4):
+        tp, tm = theta.copy(), theta.copy()
+        tp[q] += eps
+        tm[q] -= eps
+        hp, hm = build(tp).to_gpu(), build(tm).to_gpu()
+        lp, _, _ = A.adjoint_rk4(hp, [], states, 0.0, dt, S, target, forward_only=True)
+        lm, _, _ = A.adjoint_rk4(hm, [], states, 0.0, dt, S, target, forward_only=True)
+        hp.close()
+        hm.close()
+        fd = (lp[0] - lm[0]) / (2 * eps)
+        assert abs(grad[0, q] - fd) <= 1e-6 * max(abs(fd), np.abs(grad).max()), (q, grad[0, q], fd)
+    h.close()
+    ht.close()
