@@ -85,6 +85,10 @@ struct cmd_handle {
     // replayed as one graph, the executable graph updated in place per call
     cudaGraphExec_t call_graph[2] = {nullptr, nullptr};
     std::vector<unsigned char> call_sig[2];   // kernels and launch shapes of call_graph[i]
+    // streamed adjoint: one full checkpoint segment (recompute and reverse
+    // sweep) per starting order of the two cotangent buffers, keyed like stream_graph
+    cudaGraphExec_t adj_graph[2] = {nullptr, nullptr};
+    std::vector<unsigned char> adj_graph_key[2];
     cmd::DevBuf snbase;         // device step base of the replayed chunks
     std::vector<cudaEvent_t> aux_events;
     bool has_state = false;

@@ -275,6 +275,11 @@ static __global__ void stream_advance_kernel(long long* nbase, long long k) {
     if (threadIdx.x == 0 && blockIdx.x == 0) *nbase += k;
 }
 
+// Sets the step base of a replayed launch sequence.
+static __global__ void stream_set_base_kernel(long long* nbase, long long v) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *nbase = v;
+}
+
 // Observables' partials of y (the state after the last step).
 template <int NAT, int Z, int LZ>
 __global__ void __launch_bounds__(kStreamTile)
@@ -345,6 +350,7 @@ struct StreamVjpArgs {
     const double* mloc;              // [B][n_steps+1][3]
     double n_sites;
     double* gpart;                   // [B][tiles][kPart] gradient partials (accumulated)
+    const long long* nbase;          // step base of a replayed launch sequence (step = *nbase + n), or nullptr
 };
 
 // lam_b = dl_S (the loss cotangent of the last state) on every site.
@@ -367,8 +373,9 @@ __global__ void stream_lam_init_kernel(const __grid_constant__ StreamVjpArgs a, 
 template <int NAT, int Z, int LZ, int NQ>
 __global__ void __launch_bounds__(kStreamTile, 3)
 stream_vjp_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_constant__ ParamDerivs<NAT, Z, NQ> pd,
-                  const __grid_constant__ StreamVjpArgs a, int s, long long n, SVec Y, SVec lam, SVec Sprev,
+                  const __grid_constant__ StreamVjpArgs a, int s, long long n_arg, SVec Y, SVec lam, SVec Sprev,
                   double ca, double cb, SVec Sout, SVec acc, SVec lam_out, int mode) {
+    const long long n = (a.nbase ? *a.nbase : 0) + n_arg;
     __shared__ double red[32 * kRedStride];
     const int b = blockIdx.y;
     const int g = blockIdx.x * kStreamTile + threadIdx.x;    // one cell per thread

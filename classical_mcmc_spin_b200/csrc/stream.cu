@@ -243,13 +243,27 @@ int stream_adjoint(cmd_handle* h, const StreamAdjJob& j, const std::vector<doubl
     {
         const cmd::SVec y{base, V}, acc{base + B * V, V}, Ya{base + 2 * B * V, V}, Yb{base + 3 * B * V, V};
         cmd::stream_load_kernel<NAT><<<gridc, 256, 0, st>>>(j.y0, (long long)G * NAT * 3, G, y);
-        for (int64_t n = 0; n < S; ++n) {
-            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 0, n, y, y, acc, Ya, 1);
-            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 1, n, Ya, y, acc, Yb, 1);
-            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 2, n, Yb, y, acc, Ya, 1);
-            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, 3, n, Ya, y, acc, y, 1);
-            if ((n & 1023) == 0) CUDA_TRY(cudaGetLastError());
-        }
+        if (int rc = h->snbase.ensure(sizeof(long long))) return rc;
+        cmd::StreamArgs af = a;                      // steps relative to the device step base
+        af.nbase = h->snbase.as<long long>();
+        std::vector<unsigned char> key;
+        key_add(key, 2);                             // adjoint forward stages of this NAT/Z/LZ
+        key_add(key, NAT * 100 + Z * 10 + LZ);
+        key_add(key, cp);
+        key_add(key, af);
+        key_add(key, y);
+        key_add(key, acc);
+        key_add(key, Ya);
+        key_add(key, Yb);
+        key_add(key, grid);
+        auto enqueue = [&](int64_t k) {
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, af, 0, k, y, y, acc, Ya, 1);
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, af, 1, k, Ya, y, acc, Yb, 1);
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, af, 2, k, Yb, y, acc, Ya, 1);
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, af, 3, k, Ya, y, acc, y, 1);
+        };
+        int32_t nl = 0;
+        if (int rc = run_steps(h, st, S, key, enqueue, &nl)) return rc;
         cmd::stream_obs_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, a, y);
         cmd::stream_reduce_kernel<NAT><<<(unsigned)B, cmd::kStreamTile, 0, st>>>(a, S);
         CUDA_TRY(cudaGetLastError());
@@ -288,38 +302,107 @@ int stream_adjoint(cmd_handle* h, const StreamAdjJob& j, const std::vector<doubl
     double* seg = h->aseg.as<double>();
     auto slot = [&](int64_t jj, int q) { return cmd::SVec{seg + (jj * 4 + q) * V, C * 4 * V}; };
     const double dt = j.dt;
+    // One checkpoint segment of len steps: the recompute that stores every
+    // stage input, then the reverse sweep; kernel step arguments are nb + jj.
+    // The cotangent buffers l / l2 swap once per step.
+    auto segment = [&](int64_t len, int64_t nb, const cmd::StreamArgs& sa, const cmd::StreamVjpArgs& sv,
+                       cmd::SVec& l, cmd::SVec& l2) {
+        for (int64_t jj = 0; jj < len; ++jj) {
+            const int64_t n = nb + jj;
+            const cmd::SVec y = slot(jj, 0);
+            const cmd::SVec last = jj + 1 < len ? slot(jj + 1, 0) : none;
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, sa, 0, n, y, y, acc,
+                                                                                   slot(jj, 1), 0);
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, sa, 1, n, slot(jj, 1), y, acc,
+                                                                                   slot(jj, 2), 0);
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, sa, 2, n, slot(jj, 2), y, acc,
+                                                                                   slot(jj, 3), 0);
+            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, sa, 3, n, slot(jj, 3), y, acc,
+                                                                                   last, 0);
+        }
+        for (int64_t jj = len - 1; jj >= 0; --jj) {
+            const int64_t n = nb + jj;
+            auto vjp = cmd::stream_vjp_kernel<NAT, Z, LZ, NQ>;
+            vjp<<<vgrid, cmd::kStreamTile, 0, st>>>(cp, pd, sv, 3, n, slot(jj, 3), l, none, dt / 6.0, 0.0, Sa, acc,
+                                                   none, 0);
+            vjp<<<vgrid, cmd::kStreamTile, 0, st>>>(cp, pd, sv, 2, n, slot(jj, 2), l, Sa, dt / 3.0, dt, Sb, acc,
+                                                   none, 1);
+            vjp<<<vgrid, cmd::kStreamTile, 0, st>>>(cp, pd, sv, 1, n, slot(jj, 1), l, Sb, dt / 3.0, 0.5 * dt, Sa,
+                                                   acc, none, 1);
+            vjp<<<vgrid, cmd::kStreamTile, 0, st>>>(cp, pd, sv, 0, n, slot(jj, 0), l, Sa, dt / 6.0, 0.5 * dt, none,
+                                                   acc, l2, 2);
+            std::swap(l, l2);
+        }
+    };
+    // Full-length segments replay a captured graph of the segment with the
+    // kernels' steps relative to the device step base (set to the segment's
+    // first step before each replay); one graph per order of the cotangent
+    // buffers at the segment's start.  The partial segment (processed first)
+    // and, with graphs off, every segment launch directly.
+    if (int rc = h->snbase.ensure(sizeof(long long))) return rc;
+    cmd::StreamArgs ar_rel = ar;
+    ar_rel.nbase = h->snbase.as<long long>();
+    cmd::StreamVjpArgs v_rel = v;
+    v_rel.nbase = h->snbase.as<long long>();
+    const double* lam_start = lam.p;
     for (int64_t sg = K - 1; sg >= 0; --sg) {
         const int64_t n0 = sg * C, n1 = std::min(n0 + C, S);
         CUDA_TRY(cudaMemcpy2DAsync(seg, (size_t)C * 4 * V * sizeof(double), h->ackpt.as<double>() + sg * V,
                                    (size_t)K * V * sizeof(double), (size_t)V * sizeof(double), (size_t)B,
                                    cudaMemcpyDeviceToDevice, st));
-        for (int64_t n = n0; n < n1; ++n) {
-            const int64_t jj = n - n0;
-            const cmd::SVec y = slot(jj, 0);
-            const cmd::SVec last = n + 1 < n1 ? slot(jj + 1, 0) : none;
-            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, ar, 0, n, y, y, acc,
-                                                                                   slot(jj, 1), 0);
-            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, ar, 1, n, slot(jj, 1), y, acc,
-                                                                                   slot(jj, 2), 0);
-            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, ar, 2, n, slot(jj, 2), y, acc,
-                                                                                   slot(jj, 3), 0);
-            cmd::stream_stage_kernel<NAT, Z, LZ><<<grid, cmd::kStreamTile, 0, st>>>(cp, ar, 3, n, slot(jj, 3), y, acc,
-                                                                                   last, 0);
+        const int64_t len = n1 - n0;
+        if (!h->graphs || len != C || K < 3) {
+            segment(len, n0, ar, v, lam, lam2);
+            CUDA_TRY(cudaGetLastError());
+            continue;
         }
-        for (int64_t n = n1 - 1; n >= n0; --n) {
-            const int64_t jj = n - n0;
-            auto vjp = cmd::stream_vjp_kernel<NAT, Z, LZ, NQ>;
-            vjp<<<vgrid, cmd::kStreamTile, 0, st>>>(cp, pd, v, 3, n, slot(jj, 3), lam, none, dt / 6.0, 0.0, Sa, acc,
-                                                   none, 0);
-            vjp<<<vgrid, cmd::kStreamTile, 0, st>>>(cp, pd, v, 2, n, slot(jj, 2), lam, Sa, dt / 3.0, dt, Sb, acc,
-                                                   none, 1);
-            vjp<<<vgrid, cmd::kStreamTile, 0, st>>>(cp, pd, v, 1, n, slot(jj, 1), lam, Sb, dt / 3.0, 0.5 * dt, Sa, acc,
-                                                   none, 1);
-            vjp<<<vgrid, cmd::kStreamTile, 0, st>>>(cp, pd, v, 0, n, slot(jj, 0), lam, Sa, dt / 6.0, 0.5 * dt, none,
-                                                   acc, lam2, 2);
-            std::swap(lam, lam2);
-        }
+        const int par = lam.p == lam_start ? 0 : 1;
+        std::vector<unsigned char> key;
+        key_add(key, 3);                             // adjoint segment of this NAT/Z/LZ/NQ
+        key_add(key, NAT * 1000 + Z * 100 + LZ * 10 + NQ);
+        key_add(key, cp);
+        key_add(key, pd);
+        key_add(key, ar_rel);
+        key_add(key, v_rel);
+        key_add(key, lam);
+        key_add(key, lam2);
+        key_add(key, acc);
+        key_add(key, Sa);
+        key_add(key, Sb);
+        key_add(key, seg);
+        key_add(key, C);
+        key_add(key, grid);
+        key_add(key, vgrid);
+        key_add(key, dt);
+        cmd::stream_set_base_kernel<<<1, 32, 0, st>>>(h->snbase.as<long long>(), n0);
         CUDA_TRY(cudaGetLastError());
+        cudaGraphExec_t& ex = h->adj_graph[par];
+        if (!ex || h->adj_graph_key[par] != key) {
+            if (ex) {
+                cudaStreamSynchronize(st);
+                cudaGraphExecDestroy(ex);
+                ex = nullptr;
+            }
+            h->adj_graph_key[par].clear();
+            cmd::SVec l = lam, l2 = lam2;
+            cudaGraph_t g = nullptr;
+            CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            segment(len, 0, ar_rel, v_rel, l, l2);
+            const cudaError_t e = cudaStreamEndCapture(st, &g);
+            if (e != cudaSuccess || !g) {
+                if (g) cudaGraphDestroy(g);
+                return fail(CMD_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
+            }
+            const cudaError_t e2 = cudaGraphInstantiate(&ex, g, 0);
+            cudaGraphDestroy(g);
+            if (e2 != cudaSuccess) {
+                ex = nullptr;
+                return fail(CMD_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e2));
+            }
+            h->adj_graph_key[par] = key;
+        }
+        CUDA_TRY(cudaGraphLaunch(ex, st));
+        if (len & 1) std::swap(lam, lam2);
     }
     cmd::stream_grad_kernel<<<(unsigned)B, 32, 0, st>>>(v.gpart, vtiles, NQ, j.out + 1, 1 + kAdjParams);
     CUDA_TRY(cudaGetLastError());
@@ -338,6 +421,9 @@ void release_stream_graph(cmd_handle* h) {
         if (h->call_graph[i]) cudaGraphExecDestroy(h->call_graph[i]);
         h->call_graph[i] = nullptr;
         h->call_sig[i].clear();
+        if (h->adj_graph[i]) cudaGraphExecDestroy(h->adj_graph[i]);
+        h->adj_graph[i] = nullptr;
+        h->adj_graph_key[i].clear();
     }
 }
 

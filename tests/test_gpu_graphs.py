@@ -1,13 +1,14 @@
-"""CUDA graphs on the batched resident path and the uneven batch.
+"""CUDA graphs on the batched resident path, the uneven batch and the streamed adjoint.
 
 With graphs on (the default) a batched resident run (drive table, resident
 kernel, row finisher) and an uneven batch (its concurrent per-lattice launches
 and their fork / join) are captured and replayed as one graph per call, the
 handle's executable graph updated in place when only launch arguments change
-and rebuilt when the launch topology changes.  The kernels and their arguments
-are the same either way, so every result here must equal the direct launches'
-bit for bit, across calls that change pulses, batch size, step count, kernel
-variant and the set of lattices.
+and rebuilt when the launch topology changes; the streamed adjoint replays
+128-step chunks of its forward and whole checkpoint segments of its reverse
+sweep.  The kernels and their arguments are the same either way, so every
+result here must equal the direct launches' bit for bit, across calls that
+change pulses, batch size, step count, kernel variant and the set of lattices.
 """
 import numpy as np
 import pytest
@@ -104,3 +105,29 @@ def test_uneven_batch_graph_equals_direct_launches(api):
             assert list(sg) == list(sd)
     for h in hs:
         h.close()
+
+
+@pytest.mark.parametrize("ckpt", [20, 17])
+def test_streamed_adjoint_graph_equals_direct_launches(ckpt):
+    """Streamed adjoint (honeycomb 64x64, no resident kernel holds it), 300 steps: the forward replays two
+    128-step chunks, the reverse sweep replays its full checkpoint segments (even and odd segment lengths, so
+    both orders of the cotangent buffers); loss and gradient equal to direct launches bit for bit."""
+    from classical_mcmc_spin_b200 import adjoint as A
+    theta = np.array([-1.0, 0.25, -0.02, 0.05, 0.1])
+    build = lambda th: A.kitaev_lattice(th, 64, 64)
+    lat = build(theta)
+    h = lat.to_gpu()
+    B, S, dt = 2, 300, 0.01
+    states = np.stack([_spins(lat.lattice_size, 70 + b) for b in range(B)])
+    targets = np.random.default_rng(11).normal(scale=0.05, size=(B, S + 1, 3))
+    dps = A.basis_lattices(build, 5)
+    (lg, gg, mg), (ld, gd, md) = _both(h, lambda: A.adjoint_rk4(h, dps, states, 0.0, dt, S, targets,
+                                                                   checkpoint_every=ckpt, path="streamed"))
+    np.testing.assert_array_equal(lg, ld)
+    np.testing.assert_array_equal(gg, gd)
+    np.testing.assert_array_equal(mg, md)
+    # and again with graphs on: the kept graphs replay
+    l2, g2, _ = A.adjoint_rk4(h, dps, states, 0.0, dt, S, targets, checkpoint_every=ckpt, path="streamed")
+    np.testing.assert_array_equal(l2, ld)
+    np.testing.assert_array_equal(g2, gd)
+    h.close()
