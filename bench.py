@@ -215,7 +215,7 @@ def leg_uneven(torch, dev, max_steps=10000, T1=100.0, B=512):
     for k, (lat, h) in handles.items():
         gpu_api.set_tolerances(h, 1e-10, 1e-10)
         gpu_api.set_gpu_spins(h, random_unit_spins(lat.lattice_size, 2999).ravel())
-        best, _ = h.autotune_rk45(int((pick == k).sum()), 40)     # the class's own batch size: its occupancy
+        best, _ = h.autotune_rk45(int((pick == k).sum()), 200)     # the class's own batch size: its occupancy
         tilings[f"{opts[k][0]}_L{opts[k][1]}"] = next(n for i, n, _ in h.rk45_variants() if i == best)
     t_tune = time.perf_counter() - t_tune
     torch.cuda.synchronize(dev)

@@ -73,7 +73,8 @@ struct cmd_handle {
     cmd::DevBuf chunk_states, chunk_rows;   // cmd_run_batch: ping-pong states and row buffers of time chunks
     cmd::DevBuf cnbr2, cnbr4, cnbr8, cnbr16;  // partner tables of the 2-, 4-, 8- and 16-CTA cluster kernels
     cmd::DevBuf cnbr_all;       // RK45 on-chip kernels: every slot's partner word per site (built on first use)
-    int cnbr_all_cs = 0;        // cluster size cnbr_all was built for
+    cmd::DevBuf cpush;          // RK45 halo tilings: every site's push words
+    int cnbr_all_cs = 0;        // 2 * cluster size (+1 for halo words) cnbr_all / cpush were built for
     cudaStream_t copy_stream = nullptr;  // cmd_run_batch: device-to-host copies of finished chunks
     std::vector<cudaStream_t> aux_streams;   // concurrent launches of an uneven batch (created on first use)
     // streamed RK4: the stage launches of one chunk of steps captured as a CUDA

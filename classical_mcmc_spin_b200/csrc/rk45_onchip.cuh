@@ -58,6 +58,10 @@ struct R45Args {
     int G;                    // cells per trajectory
     int Gc;                   // cells per CTA
     int Gp;                   // Gc rounded up to a multiple of 32 (threads per CTA)
+    int Gs;                   // row length of the two stage buffers: Gp own cells, then (halo tilings) the
+                              // columns of partners owned by other CTAs of the cluster
+    const int* push;          // halo tilings: [G][NAT][Z-LZ] words (rank << 24) | slot in that CTA's stage
+                              // buffer 0 this site's stage inputs are pushed to, or -1
     double abs_tol, rel_tol;
     long long max_steps;      // cap on accepted steps (0: none)
     double width, freq;       // pulse envelope
@@ -68,11 +72,13 @@ struct R45Args {
 // Reduction values per warp: the observable partials padded to a power of two.
 __host__ __device__ constexpr int r45_nv(int nat) { return 3 * nat + 1 <= 8 ? 8 : 16; }
 
-// Shared memory of one CTA in doubles: two stage buffers, K2..K5 (and, with
-// yk, y and K1), the per-warp error maxima of every CTA [cs][maxt/32], rank 0's
-// per-warp observable partials [cs][maxt/32][nv] and the drive factors [12].
-__host__ __device__ constexpr long long r45_smem_doubles(int nat, int gp, int cs, int maxt, bool yk = false) {
-    return (yk ? 8LL : 6LL) * nat * 3 * gp + (long long)cs * (maxt / 32) * (1 + r45_nv(nat)) + 12;
+// Shared memory of one CTA in doubles: two stage buffers of row length gs,
+// K2..K5 (and, with yk, y and K1) of row length gp, the per-warp error maxima of
+// every CTA [cs][maxt/32], rank 0's per-warp observable partials
+// [cs][maxt/32][nv] and the drive factors [12].
+__host__ __device__ constexpr long long r45_smem_doubles(int nat, int gp, int gs, int cs, int maxt, bool yk = false) {
+    return 2LL * nat * 3 * gs + (yk ? 6LL : 4LL) * nat * 3 * gp + (long long)cs * (maxt / 32) * (1 + r45_nv(nat)) +
+           12;
 }
 
 __device__ __forceinline__ uint32_t r45_map(uint32_t local, int rank) {
@@ -121,7 +127,7 @@ __constant__ double kR45A[5][5] = {
 // product has a run-time operand, so the couplings stay constant-bank operands
 // instead of values held across the step loop: -B as z - B with z = +0 from the
 // barrier token, 2 A S as A (2 S) and -d f as d (-f) (all exact rewrites).
-template <int NAT, int Z, int LZ, int APT, int CS, bool OBS, int AG>
+template <int NAT, int Z, int LZ, int APT, int CS, bool HALO, bool OBS, int AG>
 __device__ __forceinline__ void r45_rhs_group(const Couplings<NAT, Z>& cp, const double* smem, int in, int lc,
                                               int Gp, const uint32_t (&pa)[APT][(Z - LZ) > 0 ? (Z - LZ) : 1],
                                               uint32_t tok, double f1, double f2, bool drive,
@@ -137,7 +143,7 @@ __device__ __forceinline__ void r45_rhs_group(const Couplings<NAT, Z>& cp, const
 #pragma unroll
         for (int m = 0; m < NL; ++m)
             if (LZ + m < cp.zc[at]) {
-                if constexpr (CS > 1) {
+                if constexpr (CS > 1 && !HALO) {
                     const uint32_t p0 = pa[a][m] + 8u * (uint32_t)in + tok, cs = 8u * (uint32_t)Gp;
                     P[m][0] = r45_ld_cluster(p0);
                     P[m][1] = r45_ld_cluster(p0 + cs);
@@ -204,24 +210,25 @@ __device__ __forceinline__ void r45_rhs_group(const Couplings<NAT, Z>& cp, const
 }
 
 // r45_rhs_group with the warp-uniform atom group `ag` as a compile-time constant.
-template <int NAT, int Z, int LZ, int APT, int CS, bool OBS, int AG = 0>
+template <int NAT, int Z, int LZ, int APT, int CS, bool HALO, bool OBS, int AG = 0>
 __device__ __forceinline__ void r45_rhs(int ag, const Couplings<NAT, Z>& cp, const double* smem, int in, int lc,
                                         int Gp, const uint32_t (&pa)[APT][(Z - LZ) > 0 ? (Z - LZ) : 1],
                                         uint32_t tok, double f1, double f2, bool drive, const double (&cur)[APT][3],
                                         double (&k)[APT][3], double* part) {
     if constexpr (AG + 1 < NAT / APT) {
         if (ag != AG) {
-            r45_rhs<NAT, Z, LZ, APT, CS, OBS, AG + 1>(ag, cp, smem, in, lc, Gp, pa, tok, f1, f2, drive, cur, k, part);
+            r45_rhs<NAT, Z, LZ, APT, CS, HALO, OBS, AG + 1>(ag, cp, smem, in, lc, Gp, pa, tok, f1, f2, drive, cur, k,
+                                                            part);
             return;
         }
     }
-    r45_rhs_group<NAT, Z, LZ, APT, CS, OBS, AG>(cp, smem, in, lc, Gp, pa, tok, f1, f2, drive, cur, k, part);
+    r45_rhs_group<NAT, Z, LZ, APT, CS, HALO, OBS, AG>(cp, smem, in, lc, Gp, pa, tok, f1, f2, drive, cur, k, part);
 }
 
 // Observable partials of a thread: S of its APT atoms, then S.(H - B), padded.
 __host__ __device__ constexpr int r45_nvl(int apt) { return 3 * apt + 1 <= 4 ? 4 : (3 * apt + 1 <= 8 ? 8 : 16); }
 
-template <int NAT, int Z, int LZ, int APT, int CS, int MAXT, bool YK = false>
+template <int NAT, int Z, int LZ, int APT, int CS, int MAXT, bool YK = false, bool HALO = false>
 __global__ void __launch_bounds__(MAXT, 1)
 rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_constant__ R45Args a) {
     constexpr int NL = Z - LZ;                       // bonds per atom leaving the cell
@@ -241,16 +248,18 @@ rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_co
     int rank = 0;
     if constexpr (CS > 1) rank = (int)cooperative_groups::this_cluster().block_rank();
     const GTraj& T = a.traj[blockIdx.x / CS];
-    const int Gp = a.Gp, SB = NAT * 3 * Gp;
-    double* Ks = smem + 2 * SB;                      // K2, K3, K4, K5: [4][SB], own slots
-    double* emx = smem + (YK ? 8 : 6) * SB;          // [CS][NWM] per-warp error maxima of every CTA
+    const int Gp = a.Gp, SB = NAT * 3 * Gp;          // K slots (and y, K1): rows of Gp
+    const int Gs = a.Gs, SBs = NAT * 3 * Gs;         // stage buffers: rows of Gs
+    double* Ks = smem + 2 * SBs;                     // K2, K3, K4, K5: [4][SB], own slots
+    double* emx = Ks + (YK ? 6 : 4) * SB;            // [CS][NWM] per-warp error maxima of every CTA
     double* obs = emx + CS * NWM;                    // [CS][NWM][NV] per-warp observable partials (rank 0 reads)
     double* drv = obs + CS * NWM * NV;               // [12] drive factors of stages 2..6 (pulse 1, 2)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
     const int ag = tid / Gp, lc = tid - ag * Gp;     // atom group (warp-uniform) and cell of this thread
     const int g = rank * a.Gc + lc;
     const bool own = lc < a.Gc && g < a.G;
-    const int me = ag * APT * 3 * Gp + lc;           // own slot of atom 0 of the group, component 0
+    const int me = ag * APT * 3 * Gs + lc;           // own stage-buffer slot of atom 0 of the group, component 0
+    const int mk = ag * APT * 3 * Gp + lc;           // its K slot
     const bool drive = T.pulse.a1 != 0.0 || T.pulse.a2 != 0.0;
     const double Nsites = (double)a.G * NAT;
 
@@ -263,10 +272,23 @@ rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_co
 #pragma unroll
         for (int m = 0; m < NL; ++m) {
             const int w = own ? a.pw[((long long)g * NAT + ag * APT + i) * NL + m] : ((rank << kClusterRankShift) | lc);
-            if constexpr (CS > 1)
+            if constexpr (CS > 1 && !HALO)
                 pa[i][m] = r45_map(sbase + 8u * (uint32_t)(w & kClusterOffsetMask), w >> kClusterRankShift);
             else
                 pa[i][m] = (uint32_t)(w & kClusterOffsetMask);
+        }
+    // halo tilings: shared::cluster addresses (buffer 0, component 0) of the
+    // other CTAs' halo slots this thread's sites are pushed to (~0: none)
+    uint32_t pd[APT][HALO && NL > 0 ? NL : 1];
+#pragma unroll
+    for (int i = 0; i < APT; ++i)
+#pragma unroll
+        for (int d = 0; d < (HALO && NL > 0 ? NL : 1); ++d) {
+            pd[i][d] = ~0u;
+            if constexpr (HALO) {
+                const int w = own ? a.push[((long long)g * NAT + ag * APT + i) * NL + d] : -1;
+                if (w >= 0) pd[i][d] = r45_map(sbase + 8u * (uint32_t)(w & kClusterOffsetMask), w >> kClusterRankShift);
+            }
         }
     // this warp's reduction slots
     const uint32_t emx_slot = (uint32_t)__cvta_generic_to_shared(emx + rank * NWM + warp);
@@ -276,11 +298,11 @@ rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_co
     // more shared-memory vectors, which leaves registers to the stages
     double yr[APT][3], k1r[APT][3], cur[APT][3];
     auto yref = [&](int i, int c) __attribute__((always_inline)) -> double& {
-        if constexpr (YK) return smem[6 * SB + me + (i * 3 + c) * Gp];
+        if constexpr (YK) return Ks[4 * SB + mk + (i * 3 + c) * Gp];
         else return yr[i][c];
     };
     auto k1ref = [&](int i, int c) __attribute__((always_inline)) -> double& {
-        if constexpr (YK) return smem[7 * SB + me + (i * 3 + c) * Gp];
+        if constexpr (YK) return Ks[5 * SB + mk + (i * 3 + c) * Gp];
         else return k1r[i][c];
     };
 #pragma unroll
@@ -289,21 +311,34 @@ rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_co
         for (int c = 0; c < 3; ++c) {
             yref(i, c) = own ? T.y0[((long long)g * NAT + ag * APT + i) * 3 + c] : 0.0;
             cur[i][c] = yref(i, c);
-            smem[me + (i * 3 + c) * Gp] = yref(i, c);
         }
 
     auto rhs = [&](int in, uint32_t tok, double f1, double f2, double (&k)[APT][3]) __attribute__((always_inline)) {
-        r45_rhs<NAT, Z, LZ, APT, CS, false>(ag, cp, smem, in, lc, Gp, pa, tok, f1, f2, drive, cur, k, nullptr);
+        r45_rhs<NAT, Z, LZ, APT, CS, HALO, false>(ag, cp, smem, in, lc, Gs, pa, tok, f1, f2, drive, cur, k, nullptr);
     };
     auto rhs_obs = [&](int in, uint32_t tok, double f1, double f2, double (&k)[APT][3], double (&part)[NVL])
         __attribute__((always_inline)) {
-        r45_rhs<NAT, Z, LZ, APT, CS, true>(ag, cp, smem, in, lc, Gp, pa, tok, f1, f2, drive, cur, k, part);
+        r45_rhs<NAT, Z, LZ, APT, CS, HALO, true>(ag, cp, smem, in, lc, Gs, pa, tok, f1, f2, drive, cur, k, part);
     };
-    // Publishes v as the next stage input of own atom i (registers and buffer `out`).
+    // Publishes v as the next stage input of own atom i (registers and buffer
+    // `out`; halo tilings also store it into the halo slots of the other CTAs
+    // that read it, made visible by the cluster barrier that follows).
     auto publish = [&](int out, int i, int c, double v) __attribute__((always_inline)) {
         cur[i][c] = v;
-        smem[out + me + (i * 3 + c) * Gp] = v;
+        smem[out + me + (i * 3 + c) * Gs] = v;
+        if constexpr (HALO) {
+#pragma unroll
+            for (int d = 0; d < (NL > 0 ? NL : 1); ++d)
+                if (pd[i][d] != ~0u) r45_st_cluster(pd[i][d] + 8u * (uint32_t)(out + c * Gs), v);
+        }
     };
+    // the initial state is the first stage input (halo tilings store into the
+    // other CTAs only once every CTA of the cluster runs)
+    if constexpr (HALO) r45_sync<CS>();
+#pragma unroll
+    for (int i = 0; i < APT; ++i)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) publish(0, i, c, yref(i, c));
 
     // One barrier: every warp's error maximum lands in every CTA, its observable
     // partials (placed at their atoms' rows, zeros elsewhere) in rank 0;
@@ -430,7 +465,7 @@ rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_co
                 drv[lane] = factor(lane & 1, ts);
             }
             double k[APT][3];
-            in ^= SB;
+            in ^= SBs;
 #pragma unroll
             for (int i = 0; i < APT; ++i)
 #pragma unroll
@@ -441,12 +476,12 @@ rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_co
 #pragma unroll 1
             for (int r = 0; r < 4; ++r) {
                 rhs(in, tok, drv[2 * r], drv[2 * r + 1], k);
-                in ^= SB;
+                in ^= SBs;
 #pragma unroll
                 for (int i = 0; i < APT; ++i)
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
-                        const int s = me + (i * 3 + c) * Gp;
+                        const int s = mk + (i * 3 + c) * Gp;
                         Ks[r * SB + s] = k[i][c];
                         double v = yref(i, c) + dt * kR45A[r + 1][0] * k1ref(i, c);
                         for (int j = 0; j < r; ++j) v = v + dt * kR45A[r + 1][j + 1] * Ks[j * SB + s];
@@ -456,12 +491,12 @@ rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_co
             }
             // stage 6: the new solution (published) and the first terms of the error
             rhs(in, tok, drv[8], drv[9], k);
-            in ^= SB;
+            in ^= SBs;
 #pragma unroll
             for (int i = 0; i < APT; ++i)
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
-                    const int s = me + (i * 3 + c) * Gp;
+                    const int s = mk + (i * 3 + c) * Gp;
                     const double K3 = Ks[SB + s], K4 = Ks[2 * SB + s], K5 = Ks[3 * SB + s];
                     // the partial error goes to K2's slot (K2 is not read after stage 5)
                     Ks[s] = dt * dc1 * k1ref(i, c) + dt * dc3 * K3 + dt * dc4 * K4 + dt * dc5 * K5 + dt * dc6 * k[i][c];
@@ -480,7 +515,7 @@ rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_co
             for (int i = 0; i < APT; ++i)
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
-                    const double ec = Ks[me + (i * 3 + c) * Gp] + dt * dc7 * k[i][c];
+                    const double ec = Ks[mk + (i * 3 + c) * Gp] + dt * dc7 * k[i][c];
                     const double r =
                         fabs(ec) / (a.abs_tol + a.rel_tol * (1.0 * fabs(yref(i, c)) + 1.0 * dt * fabs(k1ref(i, c))));
                     emax = fmax(emax, r);

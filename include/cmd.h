@@ -351,7 +351,9 @@ int cmd_set_graphs(cmd_handle* h, int32_t enable);
 /*
  * Tilings of the on-chip controlled Dormand-Prince kernel (CMD_RK45 in
  * cmd_integrate and cmd_run_uneven): CTAs per trajectory (one CTA or a
- * thread-block cluster of 2..16) x threads per CTA.  No reference counterpart;
+ * thread-block cluster of 2..16) x threads per CTA x sites per thread, with y
+ * and K1 in registers or shared memory ("yk") and partners in other CTAs read
+ * remotely or pushed into halo columns ("halo").  No reference counterpart;
  * the reference's controlled stepper is the CPU path's Boost.Odeint
  * make_controlled<runge_kutta_dopri5> (lattice.h:4072-4078), which every
  * tiling follows step for step.
@@ -363,9 +365,10 @@ int cmd_set_graphs(cmd_handle* h, int32_t enable);
  *   cmd_get_rk45_variant    tiling h uses now (-2: global-memory kernel)
  *   cmd_autotune_rk45       time every tiling that holds h's lattice on B
  *                           trajectories from h's current spins for n_steps
- *                           accepted steps at h's tolerances (cmd_set_tolerances),
- *                           pin the fastest; ms[cmd_rk45_variant_count()] gets
- *                           the times (-1 where a tiling does not fit), may be NULL
+ *                           accepted steps at h's tolerances (cmd_set_tolerances;
+ *                           one warm-up run, then the best of two), pin the
+ *                           fastest; ms[cmd_rk45_variant_count()] gets the times
+ *                           (-1 where a tiling does not fit), may be NULL
  */
 int cmd_rk45_variant_count(void);
 int cmd_rk45_variant_info(cmd_handle* h, int32_t idx, char* name, int32_t name_len, int32_t* fits);
