@@ -52,6 +52,9 @@ struct Layout {
     std::vector<int> slot_entry;  // [NA][Z] ELL entry at cell 0 each slot came from
     bool uniform = false;
     std::string why;            // reason when not uniform
+    // halo columns of the RK45 cluster partition into cs CTAs (index cs; -1: not
+    // computed yet), filled on first use
+    mutable std::vector<int64_t> halo_cols = std::vector<int64_t>(17, -1);
 };
 
 }  // namespace cmd

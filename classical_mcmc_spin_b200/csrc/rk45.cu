@@ -60,7 +60,9 @@ int64_t halo_columns(const Layout& L, int cs, int64_t Gc, std::vector<int>* col)
 // Row length of a tiling's stage buffers: Gp own cells, then the halo columns.
 int64_t r45_row(const R45Variant& v, const Layout& L, int64_t Gc, int64_t Gp) {
     if (!v.HALO || v.CS == 1) return Gp;
-    return Gp + (halo_columns(L, v.CS, Gc, nullptr) + 1) / 2 * 2;
+    int64_t& cols = L.halo_cols[v.CS];
+    if (cols < 0) cols = halo_columns(L, v.CS, Gc, nullptr);
+    return Gp + (cols + 1) / 2 * 2;
 }
 
 template <int NAT, int Z, int LZ, int APT, int CS, int MAXT, bool YK, bool HALO>
