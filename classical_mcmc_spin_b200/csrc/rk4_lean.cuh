@@ -9,7 +9,7 @@
 //   * four stages per step alternate the two buffers, so the buffer a stage
 //     reads is known at compile time: each partner's address is resolved once,
 //     before the loop, and the other buffer is a compile-time offset from it;
-//   * every atom carries Z bonds (checked on the host).  The per-slot test of
+//   * every atom carries Z bonds (checked on the host).  A per-atom test of
 //     the bond count stays in the loop all the same: it is a uniform branch,
 //     and without it the compiler moves the coupling loads out of the step
 //     loop into registers and spills.
@@ -99,9 +99,9 @@ rk4_lean_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_const
                 bond_acc(H[d], cp.J[at][n][3 * d], cp.J[at][n][3 * d + 1], cp.J[at][n][3 * d + 2], S[pa][0],
                          S[pa][1], S[pa][2]);
         }
+        if (LZ >= cp.zc[at]) return;                  // always false here; keeps the couplings operands
 #pragma unroll
         for (int m = 0; m < NL; ++m) {
-            if (LZ + m >= cp.zc[at]) continue;         // always false here; keeps the couplings operands
             const double* p = smem + (pb[at][m] + buf * SB);
             const double P0 = p[0], P1 = p[GS], P2 = p[2 * GS];
 #pragma unroll
