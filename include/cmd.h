@@ -341,8 +341,11 @@ int cmd_autotune(cmd_handle* h, int64_t B, int64_t n_steps, int32_t* best, doubl
  * uneven batches (the per-lattice launches on the handle's auxiliary streams,
  * forked from and joined to the call's stream): each call is captured and
  * launched as one graph, the handle's executable graph updated in place when
- * only arguments change.  Calls on a default stream, or on a stream the caller
- * is capturing, launch directly.  The results are the same either way.  No
+ * only arguments change.  Calls on a default stream launch directly.  The
+ * library does not capture a stream that is already being captured; its calls
+ * also upload host data (time grids, trajectory tables) with ordinary copies,
+ * so they are not meant to be recorded into a caller's own graph.  The results
+ * are the same with graphs on or off.  No
  * reference counterpart (the reference launches and synchronises every stage,
  * integrator.cuh:115-139).  enable = 0 launches everything directly.
  */
