@@ -251,7 +251,9 @@ int rk45_launch(cmd_handle* h, int variant, const GTraj* d_traj, int64_t B, doub
     a.push = v.HALO ? h->cpush.as<int>() : nullptr;
     a.abs_tol = abs_tol;
     a.rel_tol = rel_tol;
-    a.max_steps = max_steps;
+    // the kernel counts accepted steps in 32 bits: "no cap" becomes 2^31 - 2
+    constexpr int64_t kMaxCap = 2147483646;
+    a.max_steps = (int)((max_steps <= 0 || max_steps > kMaxCap) ? kMaxCap : max_steps);
     a.width = h->width;
     a.freq = h->freq;
     a.frames = h->dframes.as<double>();

@@ -63,7 +63,7 @@ struct R45Args {
     const int* push;          // halo tilings: [G][NAT][Z-LZ] words (rank << 24) | slot in that CTA's stage
                               // buffer 0 this site's stage inputs are pushed to, or -1
     double abs_tol, rel_tol;
-    long long max_steps;      // cap on accepted steps (0: none)
+    int max_steps;            // cap on accepted steps, 1 .. 2^31 - 2 (the host turns "none" into the largest)
     double width, freq;       // pulse envelope
     const double* frames;     // [NAT*9] (device)
     const double* afm;        // [NAT]
@@ -381,13 +381,13 @@ rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_co
         return err;
     };
 
-    long long nrow = 0;
+    int nrow = 0;                                    // 32-bit counters: fewer registers held across the steps
     // Row nrow = {t, M_af, M_local, M_global, E/N} from the observable sums held
     // by rank 0's warp 0 (lane q: observable q); states of the row if saved.
     auto record = [&](double t, double obs_q) __attribute__((always_inline)) {
         if (nrow < T.max_rows) {
             if (T.traj && own) {
-                double* dst = T.traj + nrow * (long long)a.G * NAT * 3 + ((long long)g * NAT + ag * APT) * 3;
+                double* dst = T.traj + (long long)nrow * a.G * NAT * 3 + ((long long)g * NAT + ag * APT) * 3;
 #pragma unroll
                 for (int i = 0; i < APT; ++i)
 #pragma unroll
@@ -411,7 +411,7 @@ rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_co
                             ma[d] += a.afm[a2] * v;
                         }
                     }
-                    double* o = T.rows + nrow * 11;
+                    double* o = T.rows + (long long)nrow * 11;
                     o[0] = t;
 #pragma unroll
                     for (int d = 0; d < 3; ++d) {
@@ -451,7 +451,8 @@ rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_co
         record(t, obs_q);
     }
 
-    long long acc_steps = 0, rej_steps = 0, status = 0;
+    int acc_steps = 0, status = 0;
+    long long rej_steps = 0;
     double dt = T.dt0;
     while (T.T1 - t > eps) {
         if ((t + dt) - T.T1 > eps) dt = T.T1 - t;
@@ -553,7 +554,7 @@ rk45_onchip_kernel(const __grid_constant__ Couplings<NAT, Z> cp, const __grid_co
             break;
         }
         if (status != 0) break;
-        if (a.max_steps > 0 && acc_steps >= a.max_steps) break;
+        if (acc_steps >= a.max_steps) break;
     }
     if (T.yout && own)
 #pragma unroll
