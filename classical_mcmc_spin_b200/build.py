@@ -77,7 +77,7 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
         raise RuntimeError(f"{len(failed)} source(s) failed to compile")
     objs = [str(BUILD / (Path(src).stem + ".o")) for src in SOURCES]
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart", "-lcufft"]
+    cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart", "-lcufft", "-lpthread"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)

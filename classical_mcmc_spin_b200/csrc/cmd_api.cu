@@ -14,6 +14,7 @@
 #include "rk_global.cuh"
 
 #include <chrono>
+#include <thread>
 #include <cmath>
 #include <cstdio>
 
@@ -400,6 +401,7 @@ int cmd_destroy(cmd_handle* h) {
                       &h->awork, &h->ackpt, &h->aseg, &h->amloc, &h->aout, &h->ameta, &h->ain,
                       &h->sbuf, &h->spart, &h->sgpart, &h->snbase, &h->chunk_states, &h->chunk_rows, &h->cnbr2, &h->cnbr4, &h->cnbr8, &h->cnbr16, &h->cnbr_all, &h->cpush})
         b->release();
+    h->hstage.release();
     for (cudaStream_t s2 : h->aux_streams) cudaStreamSynchronize(s2);
     for (cudaEvent_t e2 : h->aux_events) cudaEventDestroy(e2);
     for (cudaStream_t s2 : h->aux_streams) cudaStreamDestroy(s2);
@@ -661,17 +663,51 @@ int cmd_run_uneven(cmd_traj_spec* specs, int64_t B, int method, double abs_tol, 
     std::vector<long long> stats;
     if (int rc = run_global(owner, jobs, mode_of(method), abs_tol, rel_tol, max_steps, stats)) return rc;
     bool overflow = false;
+    // Rows and final states: device -> page-locked staging (one asynchronous copy
+    // each), then into the caller's arrays on a few host threads; where the
+    // staging cannot be had, straight into the caller's arrays.
+    std::vector<size_t> hoff(B), foff(B);
+    size_t hs_total = 0;
     for (int64_t b = 0; b < B; ++b) {
         cmd_traj_spec& sp = specs[b];
         for (int q = 0; q < 4; ++q) sp.stats[q] = stats[4 * b + q];
-        const int64_t n = std::min<int64_t>(sp.stats[0], sp.max_rows);
         overflow |= sp.stats[0] > sp.max_rows;
-        CUDA_TRY(cudaMemcpyAsync(sp.rows, drows + roff[b], n * 11 * sizeof(double), cudaMemcpyDeviceToHost, owner->stream));
+        hoff[b] = hs_total;
+        hs_total += (size_t)std::min<int64_t>(sp.stats[0], sp.max_rows) * 11;
+    }
+    for (int64_t b = 0; b < B; ++b) {
+        foff[b] = hs_total;
+        if (specs[b].final_state) hs_total += (size_t)specs[b].lattice->N * 3;
+    }
+    const bool staged = owner->hstage.ensure(std::max<size_t>(hs_total, 1) * sizeof(double)) == CMD_OK;
+    cmd::clear_error();
+    double* hst = staged ? owner->hstage.as<double>() : nullptr;
+    for (int64_t b = 0; b < B; ++b) {
+        cmd_traj_spec& sp = specs[b];
+        const int64_t n = std::min<int64_t>(sp.stats[0], sp.max_rows);
+        CUDA_TRY(cudaMemcpyAsync(staged ? hst + hoff[b] : sp.rows, drows + roff[b], n * 11 * sizeof(double),
+                                 cudaMemcpyDeviceToHost, owner->stream));
         if (sp.final_state)
-            CUDA_TRY(cudaMemcpyAsync(sp.final_state, dout + ioff[b], sp.lattice->N * 3 * sizeof(double),
-                                     cudaMemcpyDeviceToHost, owner->stream));
+            CUDA_TRY(cudaMemcpyAsync(staged ? hst + foff[b] : sp.final_state, dout + ioff[b],
+                                     sp.lattice->N * 3 * sizeof(double), cudaMemcpyDeviceToHost, owner->stream));
     }
     if (int rc = sync(owner)) return rc;
+    if (staged) {
+        const int nt = (int)std::max<int64_t>(1, std::min<int64_t>(B, 8));
+        auto part = [&](int k) {
+            for (int64_t b = k; b < B; b += nt) {
+                cmd_traj_spec& sp = specs[b];
+                const int64_t n = std::min<int64_t>(sp.stats[0], sp.max_rows);
+                std::memcpy(sp.rows, hst + hoff[b], (size_t)n * 11 * sizeof(double));
+                if (sp.final_state)
+                    std::memcpy(sp.final_state, hst + foff[b], (size_t)sp.lattice->N * 3 * sizeof(double));
+            }
+        };
+        std::vector<std::thread> pool;
+        for (int k = 1; k < nt; ++k) pool.emplace_back(part, k);
+        part(0);
+        for (std::thread& t : pool) t.join();
+    }
     if (overflow) return fail(CMD_ERR_INVALID_ARG, "max_rows too small for some trajectory");
     for (int64_t b = 0; b < B; ++b)
         if (specs[b].stats[3] != 0) return fail(CMD_ERR_NONFINITE, "step-size control failed for some trajectory");

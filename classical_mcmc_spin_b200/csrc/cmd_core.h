@@ -79,6 +79,7 @@ struct cmd_handle {
     cmd::DevBuf cpush;          // RK45 halo tilings: every site's push words
     int cnbr_all_cs = 0;        // 2 * cluster size (+1 for halo words) cnbr_all / cpush were built for
     cudaStream_t copy_stream = nullptr;  // cmd_run_batch: device-to-host copies of finished chunks
+    cmd::HostBuf hstage;        // cmd_run_uneven: page-locked staging of the rows and final states
     std::vector<cudaStream_t> aux_streams;   // concurrent launches of an uneven batch (created on first use)
     // streamed RK4: the stage launches of one chunk of steps captured as a CUDA
     // graph, replayed per chunk; rebuilt when any launch parameter changes

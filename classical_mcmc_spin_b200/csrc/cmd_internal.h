@@ -39,4 +39,30 @@ struct DevBuf {
     template <class T> T* as() const { return static_cast<T*>(p); }
 };
 
+// Page-locked host buffer, grown on demand (device-to-host copies into it run
+// at full link speed and asynchronously).
+struct HostBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t n) {
+        if (n <= bytes) return CMD_OK;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaHostAlloc(&p, n, cudaHostAllocDefault);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return fail(CMD_ERR_OOM, std::string("cudaHostAlloc: ") + cudaGetErrorString(e));
+        }
+        bytes = n;
+        return CMD_OK;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
 }  // namespace cmd
