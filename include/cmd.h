@@ -252,9 +252,15 @@ int cmd_layout_info(cmd_handle* h, int64_t* info);
 /*
  * Uneven batch (no reference counterpart): trajectories on different lattices
  * (different sizes, and up to two unit-cell types, e.g. Kitaev honeycomb and
- * non-Kramers pyrochlore) in ONE persistent launch that pulls trajectories
- * from a work queue, longest first.  Lattices of one unit-cell type must share
- * their couplings, pulse directions, width and frequency (cmd_set_pulse).
+ * non-Kramers pyrochlore) in one call.  Controlled RK45 runs each lattice's
+ * trajectories on the on-chip Dormand-Prince kernel with that handle's tiling
+ * (cmd_set_rk45_variant / cmd_autotune_rk45), the lattices' launches running
+ * concurrently; everything else runs in one persistent launch that pulls
+ * trajectories from a work queue, longest first.  Lattices of one unit-cell
+ * type must share their couplings, pulse directions, width and frequency
+ * (cmd_set_pulse).  The rows and final states come back through a page-locked
+ * host buffer held by the first spec's handle (as large as the rows returned;
+ * kept for later calls and freed by cmd_destroy).
  * method: CMD_RK45 (controlled, T0..T1 from dt, tolerances below, at most
  * max_steps accepted steps when > 0; a row after every accepted step) or
  * CMD_RK4 / CMD_DOPRI5_FIXED (fixed dt, reference loop, a row every step).
