@@ -328,11 +328,17 @@ def run_uneven(specs, method="rk45", abs_tol=1e-10, rel_tol=1e-10, max_steps=0):
     B = len(specs)
     arr = (nat.TrajSpec * B)()
     keep = []
+    mrs = [int(sp.get("max_rows", (max_steps + 2) if max_steps else int((sp["T1"] - sp["T0"]) / sp["dt"]) + 2))
+           for sp in specs]
+    # one block for every trajectory's rows (views per trajectory): a large allocation is backed by huge pages,
+    # so filling it costs far fewer page faults than many small arrays
+    block = np.empty((sum(mrs), 11))
+    offs = np.concatenate(([0], np.cumsum(mrs)))
     for b, sp in enumerate(specs):
         h = sp["handle"]
         st = f64(sp["state"], 3 * h.N)
-        mr = int(sp.get("max_rows", (max_steps + 2) if max_steps else int((sp["T1"] - sp["T0"]) / sp["dt"]) + 2))
-        rows = np.zeros((mr, 11))
+        mr = mrs[b]
+        rows = block[offs[b]:offs[b] + mr]
         fin = np.zeros(3 * h.N) if sp.get("want_final", True) else None
         keep.append((st, rows, fin))
         a = arr[b]
